@@ -1,0 +1,178 @@
+// C ABI (include/fherma_polymult.h) and the reference's C++ entry points
+// (include/fherma_abi.h) over fpm::Engine.
+#include "fherma_abi.h"
+#include "fherma_polymult.h"
+
+#include "engine.h"
+#include "kernels.h"
+
+#include <cuda_runtime.h>
+
+#include <exception>
+#include <new>
+#include <stdexcept>
+#include <string>
+
+struct fpm_ctx {
+    fpm::Engine* engine;
+    uint32_t W;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg) {
+    g_error = msg;
+    return code;
+}
+
+// Runs f, mapping exceptions to error codes.
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        return FPM_OK;
+    } catch (const std::bad_alloc&) {
+        return fail(FPM_ENOMEM, "out of host memory");
+    } catch (const fpm::CudaError& e) {
+        return fail(e.code == cudaErrorMemoryAllocation ? FPM_ENOMEM : FPM_ECUDA, e.what());
+    } catch (const std::runtime_error& e) {
+        return fail(FPM_EINVAL, e.what());
+    } catch (const std::exception& e) {
+        return fail(FPM_EINTERNAL, e.what());
+    }
+}
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+extern "C" {
+
+const char* fpm_last_error(void) { return g_error.c_str(); }
+
+int fpm_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, fpm_ctx** out) {
+    if (!out) return fail(FPM_EINVAL, "fpm_init: out is NULL");
+    *out = nullptr;
+    if (!q) return fail(FPM_EINVAL, "fpm_init: q is NULL");
+    if (L < 1 || L > static_cast<uint32_t>(fpm::kMaxL))
+        return fail(FPM_EINVAL, "L must be in [1, " + std::to_string(fpm::kMaxL) + "]; got " + std::to_string(L));
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(FPM_ECUDA, "no CUDA device: this library has no CPU fallback");
+    }
+    fpm::Engine* e = nullptr;
+    const int rc = guarded([&] { e = new fpm::Engine(N, W, q, static_cast<int>(L)); });
+    if (rc) return rc;
+    *out = new fpm_ctx{e, W};
+    return FPM_OK;
+}
+
+int fpm_run(fpm_ctx* ctx, const uint32_t* a, const uint32_t* b, uint32_t* c) {
+    if (!ctx || !a || !b || !c) return fail(FPM_EINVAL, "fpm_run: NULL argument");
+    return guarded([&] { ctx->engine->run_host(a, b, c); });
+}
+
+int fpm_run_device(fpm_ctx* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, void* stream) {
+    if (!ctx || !d_a || !d_b || !d_c) return fail(FPM_EINVAL, "fpm_run_device: NULL argument");
+    return guarded([&] { ctx->engine->run_device(d_a, d_b, d_c, as_stream(stream)); });
+}
+
+void fpm_free(fpm_ctx* ctx) {
+    if (!ctx) return;
+    delete ctx->engine;
+    delete ctx;
+}
+
+int fpm_get_info(const fpm_ctx* ctx, fpm_info* out) {
+    if (!ctx || !out) return fail(FPM_EINVAL, "fpm_get_info: NULL argument");
+    const fpm::HostPlan& pl = ctx->engine->plan();
+    out->N = pl.N;
+    out->W = ctx->W;
+    out->L = static_cast<uint32_t>(pl.L);
+    out->K = static_cast<uint32_t>(pl.K);
+    out->logN = pl.g.logN;
+    out->logR = pl.g.logR;
+    out->logS = pl.g.logS;
+    out->device = ctx->engine->device();
+    out->device_bytes = fpm::device_footprint(pl);
+    return FPM_OK;
+}
+
+int fpm_plan_info(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, fpm_info* out, uint32_t* primes) {
+    if (!q || !out) return fail(FPM_EINVAL, "fpm_plan_info: NULL argument");
+    return guarded([&] {
+        const fpm::HostPlan pl = fpm::make_plan(N, W, q, static_cast<int>(L));
+        out->N = pl.N;
+        out->W = W;
+        out->L = static_cast<uint32_t>(pl.L);
+        out->K = static_cast<uint32_t>(pl.K);
+        out->logN = pl.g.logN;
+        out->logR = pl.g.logR;
+        out->logS = pl.g.logS;
+        out->device = -1;
+        out->device_bytes = fpm::device_footprint(pl);
+        if (primes) {
+            for (int j = 0; j < pl.K; ++j) primes[j] = pl.primes[j];
+        }
+    });
+}
+
+int fpm_get_primes(const fpm_ctx* ctx, uint32_t* out) {
+    if (!ctx || !out) return fail(FPM_EINVAL, "fpm_get_primes: NULL argument");
+    const auto& p = ctx->engine->plan().primes;
+    for (size_t i = 0; i < p.size(); ++i) out[i] = p[i];
+    return FPM_OK;
+}
+
+int fpm_stage_decompose(fpm_ctx* ctx, const uint32_t* d_limbs, uint32_t* d_res, int operand, void* stream) {
+    if (!ctx || !d_limbs || !d_res || (operand != 0 && operand != 1))
+        return fail(FPM_EINVAL, "fpm_stage_decompose: bad argument");
+    return guarded([&] { ctx->engine->decompose(d_limbs, d_res, operand, as_stream(stream)); });
+}
+
+int fpm_stage_transform(fpm_ctx* ctx, uint32_t* d_A, uint32_t* d_B, int mode, void* stream) {
+    if (!ctx || !d_A || !d_B || (mode != 0 && mode != 1))
+        return fail(FPM_EINVAL, "fpm_stage_transform: bad argument");
+    return guarded([&] { ctx->engine->transform(d_A, d_B, mode, as_stream(stream)); });
+}
+
+int fpm_stage_crt(fpm_ctx* ctx, const uint32_t* d_y, uint32_t* d_c, void* stream) {
+    if (!ctx || !d_y || !d_c) return fail(FPM_EINVAL, "fpm_stage_crt: bad argument");
+    return guarded([&] { ctx->engine->crt(d_y, d_c, as_stream(stream)); });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// The reference's C++ entry points (fherma.h:46-48).
+
+void* fherma_init(const fherma::Point& p) {
+    if (p.q.data.size() != p.L) {
+        throw std::runtime_error("q has " + std::to_string(p.q.data.size()) + " limbs, expected L = " +
+                                 std::to_string(p.L));
+    }
+    fpm_ctx* ctx = nullptr;
+    if (fpm_init(p.N, p.W, p.L, p.q.data.data(), &ctx) != FPM_OK) throw std::runtime_error(fpm_last_error());
+    return ctx;
+}
+
+fherma::Outputs fherma_run(void* state, const fherma::Inputs& in) {
+    auto* ctx = static_cast<fpm_ctx*>(state);
+    if (!ctx) throw std::runtime_error("fherma_run: null state");
+    const fpm::HostPlan& pl = ctx->engine->plan();
+    const size_t words = static_cast<size_t>(pl.N) * pl.L;
+    if (in.a.data.size() != words || in.b.data.size() != words) {
+        throw std::runtime_error("operand size does not match the point");
+    }
+    fherma::Outputs out;
+    out.c.shape = {static_cast<int64_t>(pl.N), static_cast<int64_t>(pl.L)};
+    out.c.data.resize(words);
+    if (fpm_run(ctx, in.a.data.data(), in.b.data.data(), out.c.data.data()) != FPM_OK)
+        throw std::runtime_error(fpm_last_error());
+    return out;
+}
+
+void fherma_free(void* state) { fpm_free(static_cast<fpm_ctx*>(state)); }

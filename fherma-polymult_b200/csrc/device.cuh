@@ -1,0 +1,39 @@
+// Device-side description of one product's point: sizes, and pointers into
+// the device copies of the HostPlan tables (plan.h).  Passed to kernels by
+// value.  Residue buffers are K x N u32, prime-major: X[j * N + n].
+#pragma once
+
+#include "arith.cuh"
+
+#include <cstdint>
+
+namespace fpm {
+
+struct DevPoint {
+    uint32_t N, logN, logR, logS;
+    int L, K;
+    const PrimeConsts* pc;     // K
+    const uint2* dec_a;        // K x L
+    const uint2* dec_b;        // K x L
+    const uint2* col_f;        // K x R
+    const uint2* col_i;
+    const uint2* row_u_f;      // K x R x logS
+    const uint2* row_u_i;
+    const uint2* row_q_f;      // K x S
+    const uint2* row_q_i;
+    const uint2* full_f;       // K x N (small transforms)
+    const uint2* full_i;
+    const uint32_t* q;         // L
+    double q_top;
+    const uint32_t* M;         // K x L
+    const uint32_t* negvP;     // (K + 1) x L
+    const double* p_recip;     // K
+};
+
+// What the row kernel does with its tile.
+enum RowMode : int {
+    kRowProduct = 0,   // forward rows of A and B, pointwise A B, inverse rows -> A
+    kRowForward = 1,   // forward rows of A and B only (for stage checks)
+};
+
+}  // namespace fpm

@@ -1,0 +1,70 @@
+// One point's resident state on one GPU: the plan tables in device memory,
+// residue workspaces, pinned staging and the launch sequence of a product.
+#pragma once
+
+#include "device.cuh"
+#include "plan.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+namespace fpm {
+
+class Engine {
+public:
+    // Builds the plan and uploads it (throws std::runtime_error).
+    Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2 = 31);
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    const HostPlan& plan() const { return plan_; }
+    const DevPoint& point() const { return dp_; }
+    int device() const { return device_; }
+
+    // c = a b on device buffers (N x L each), enqueued on st; the engine's
+    // residue workspaces are used, so calls on one engine must not overlap.
+    void run_device(const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t st);
+
+    // c = a b on host buffers (pageable or not, N x L each); returns when c is
+    // written.
+    void run_host(const uint32_t* a, const uint32_t* b, uint32_t* c);
+
+    // Stages, for checks against the oracle.
+    void decompose(const uint32_t* d_limbs, uint32_t* d_res, int operand, cudaStream_t st);
+    void transform(uint32_t* d_A, uint32_t* d_B, int mode, cudaStream_t st);
+    void crt(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st);
+
+    size_t words() const { return static_cast<size_t>(plan_.N) * plan_.L; }
+    size_t residues() const { return static_cast<size_t>(plan_.K) * plan_.N; }
+
+private:
+    void release();
+    template <class T>
+    T* dalloc(size_t count);
+    template <class T>
+    const T* upload(const std::vector<T>& v);
+
+    HostPlan plan_;
+    DevPoint dp_{};
+    int device_ = 0;
+    std::vector<void*> dmem_;
+    uint32_t* A_ = nullptr;   // K x N residues
+    uint32_t* B_ = nullptr;
+    uint32_t* la_ = nullptr;  // N x L device limbs for the host path
+    uint32_t* lb_ = nullptr;
+    uint32_t* lc_ = nullptr;
+    uint32_t* ha_ = nullptr;  // pinned staging
+    uint32_t* hb_ = nullptr;
+    uint32_t* hc_ = nullptr;
+    cudaStream_t stream_ = nullptr;
+    cudaStream_t copy_ = nullptr;
+    std::vector<cudaEvent_t> events_;
+};
+
+// Shared-memory opt-ins, once per device per process.
+void ensure_kernel_attributes(int device);
+
+}  // namespace fpm

@@ -1,0 +1,49 @@
+// Host-side launch interface of the kernels.
+#pragma once
+
+#include "device.cuh"
+#include "plan.h"
+
+#include <cuda_runtime.h>
+
+#include <stdexcept>
+#include <string>
+
+namespace fpm {
+
+// A failed CUDA call ("<what>: <CUDA message>").  Invalid points and other
+// argument errors are plain std::runtime_error.
+struct CudaError : std::runtime_error {
+    cudaError_t code;
+    CudaError(const std::string& msg, cudaError_t c) : std::runtime_error(msg), code(c) {}
+};
+
+inline void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e), e);
+}
+
+// Columns per column-pass tile of 2048 elements.
+template <int LOGR>
+constexpr uint32_t kTileCols = 2048u >> LOGR;
+
+size_t col_fwd_smem(uint32_t logR);
+size_t col_inv_smem(uint32_t logR);
+size_t row_smem();
+
+// One-time per process: shared-memory opt-ins for the kernels.
+void ntt_init_attributes();
+void decompose_init_attributes();
+void crt_init_attributes();
+
+// limbs (N x L, coefficient-major) -> residues (K x N); operand 1 (b) is
+// scaled for the pointwise step.
+void launch_decompose(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, cudaStream_t st);
+
+// Residues A, B -> y_j in A (mode kRowProduct), or the forward transforms of
+// both in place (mode kRowForward).
+void launch_ntt(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStream_t st);
+
+// y_j (K x N) -> c (N x L) mod q.
+void launch_crt(const DevPoint& d, const uint32_t* Y, uint32_t* c, cudaStream_t st);
+
+}  // namespace fpm

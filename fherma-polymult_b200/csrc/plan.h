@@ -1,0 +1,80 @@
+// Host-side setup for one point (N, q): the prime set and every constant table
+// the kernels read.  Built once per point, outside any timed call.
+//
+// Reference counterpart: rns_plan.h:118-280 (make_plan, add_full_twiddles,
+// use_gen_twiddles).  The prime set, the choice of each prime's root psi_j and
+// the CRT constants follow the reference exactly (same primes in the same
+// order, so residues compare stage by stage with the oracle); the twiddle
+// tables are laid out for this library's kernels instead.
+#pragma once
+
+#include "arith.cuh"
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace fpm {
+
+// How the length-N transform is cut for the kernels.
+//   logN <= kSmallLogN : one block per prime holds the whole transform
+//                        (k_ntt_small), full twiddle tables.
+//   logN == 11         : one 2048-element tile per prime (row kernel, R = 1).
+//   logN >= 12         : four-step, N = R x S with S = 2^ceil(logN/2):
+//                        column pass (stages of distance >= S, along the R
+//                        rows of each column) and row pass (distance < S).
+constexpr uint32_t kSmallLogN = 10;
+constexpr uint32_t kTileLog = 11;            // 2048-element tiles
+constexpr uint32_t kTile = 1u << kTileLog;
+
+struct Geometry {
+    uint32_t logN = 0, logR = 0, logS = 0;
+    bool small = false;
+};
+
+Geometry make_geometry(uint32_t logN);
+
+struct HostPlan {
+    uint32_t N = 0, W = 0;
+    int L = 0, K = 0;
+    Geometry g;
+    std::vector<uint32_t> q;      // L
+    double q_top = 0;             // top limbs of q as a double
+    int pmax_log2 = 31;
+
+    std::vector<uint32_t> primes;            // K
+    std::vector<PrimeConsts> pc;             // K
+    std::vector<uint32_t> psi, ipsi;         // K
+
+    // Decompose: x mod p_j = sum_l x_l c_{j,l}.  a uses c = 2^(32 l) mod p_j;
+    // b folds in the pointwise scale N^-1 (P/p_j)^-1 2^32 (the 2^32 undoes the
+    // Montgomery product in the pointwise step), so the inverse transform ends
+    // in y_j directly.  K x L Shoup pairs each.
+    std::vector<uint2> dec_a, dec_b;
+
+    // Column pass twiddles (logN >= 12): psi^(S bitrev_logR(y)) for y in [1, R),
+    // K x R pairs (entry 0 unused); inverse with psi^-1.
+    std::vector<uint2> col_f, col_i;
+    // Row pass twiddle generators: the twiddle of stage b (distance 2^b) for
+    // row u and group r' is psi^(2^b (1 + 2 bitrev_logR(u)) + 2^(b+1+logR) bitrev(r')),
+    // = U[u][b] * Q[y] with y = 2^(logS-1-b) + r'.
+    //   row_u_*: K x R x logS pairs, row_q_*: K x S pairs (entry 0 unused).
+    std::vector<uint2> row_u_f, row_u_i, row_q_f, row_q_i;
+    // Small transforms (logN <= kSmallLogN): psi^bitrev_logN(y), K x N pairs.
+    std::vector<uint2> full_f, full_i;
+
+    // CRT: M_j = P / p_j mod q (K x L), negvP_v = -v P mod q ((K + 1) x L),
+    // 1 / p_j (K).
+    std::vector<uint32_t> M, negvP;
+    std::vector<double> p_recip;
+};
+
+// Device bytes an Engine for this plan holds (tables, residue workspaces and
+// the limb buffers of the host path).
+size_t device_footprint(const HostPlan& pl);
+
+// Throws std::runtime_error on an out-of-range point (N not a power of two in
+// [2, 2^22], L outside [1, 64], q's top limb zero, not enough primes).
+HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2 = 31);
+
+}  // namespace fpm

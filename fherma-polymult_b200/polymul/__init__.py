@@ -1,0 +1,205 @@
+"""Python mirror of the reference's plugin interface, over the C ABI of
+lib/libfpm.so (include/fherma_polymult.h).
+
+The reference's solution is three C++ functions bound by the FHERMA harness
+(fherma.h:46-48):
+
+    void*           fherma_init(const fherma::Point&)
+    fherma::Outputs fherma_run(void* state, const fherma::Inputs&)
+    void            fherma_free(void* state)
+
+This module offers the same three names with the same argument meaning and the
+same error behaviour (an out-of-range point or a mis-sized operand raises, as
+the reference throws std::runtime_error), taking numpy arrays in place of
+fherma::Tensor.  ``Context`` exposes the rest of the C ABI: products on device
+buffers enqueued on a CUDA stream, the stage entry points, and the host-only
+plan query.
+
+There is no CPU fallback: loading fails if lib/libfpm.so is missing, and
+fherma_init fails without a CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libfpm.so")
+
+FPM_OK, FPM_EINVAL, FPM_ECUDA, FPM_ENOMEM, FPM_EINTERNAL = 0, 1, 2, 3, 4
+MODE_PRODUCT, MODE_FORWARD = 0, 1
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+
+
+class FpmInfo(ctypes.Structure):
+    _fields_ = [("N", ctypes.c_uint32), ("W", ctypes.c_uint32), ("L", ctypes.c_uint32), ("K", ctypes.c_uint32),
+                ("logN", ctypes.c_uint32), ("logR", ctypes.c_uint32), ("logS", ctypes.c_uint32),
+                ("device", ctypes.c_int32), ("device_bytes", ctypes.c_uint64)]
+
+
+class FpmError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(message)
+        self.code = code
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads lib/libfpm.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `make -C fherma-polymult_b200` "
+                           "(there is no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    sig = {
+        "fpm_init": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u32p, ctypes.POINTER(vp)], ctypes.c_int),
+        "fpm_run": ([vp, vp, vp, vp], ctypes.c_int),
+        "fpm_run_device": ([vp, vp, vp, vp, vp], ctypes.c_int),
+        "fpm_free": ([vp], None),
+        "fpm_last_error": ([], ctypes.c_char_p),
+        "fpm_get_info": ([vp, ctypes.POINTER(FpmInfo)], ctypes.c_int),
+        "fpm_plan_info": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u32p, ctypes.POINTER(FpmInfo), _u32p],
+                          ctypes.c_int),
+        "fpm_get_primes": ([vp, _u32p], ctypes.c_int),
+        "fpm_stage_decompose": ([vp, vp, vp, ctypes.c_int, vp], ctypes.c_int),
+        "fpm_stage_transform": ([vp, vp, vp, ctypes.c_int, vp], ctypes.c_int),
+        "fpm_stage_crt": ([vp, vp, vp, vp], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _check(rc: int):
+    if rc != FPM_OK:
+        raise FpmError(rc, load().fpm_last_error().decode())
+
+
+def _limbs(x, rows: int, L: int, name: str) -> np.ndarray:
+    x = np.ascontiguousarray(x, dtype=np.uint32)
+    if x.size != rows * L:
+        # reference solve.cu:877-879: "operand size does not match the point"
+        raise FpmError(FPM_EINVAL, f"{name}: operand size does not match the point")
+    return x.reshape(rows, L)
+
+
+def plan_info(N: int, W: int, q) -> tuple[FpmInfo, np.ndarray]:
+    """Host-only: the plan fherma_init would build (raises on a bad point)."""
+    lib = load()
+    q = np.ascontiguousarray(q, dtype=np.uint32)
+    info = FpmInfo()
+    primes = np.zeros(160, np.uint32)
+    _check(lib.fpm_plan_info(N, W, q.shape[0], q.ctypes.data_as(_u32p), ctypes.byref(info),
+                             primes.ctypes.data_as(_u32p)))
+    return info, primes[:info.K].copy()
+
+
+class Context:
+    """One point's resident state on the current CUDA device (fpm_ctx)."""
+
+    def __init__(self, N: int, W: int, q):
+        lib = load()
+        q = np.ascontiguousarray(q, dtype=np.uint32)
+        h = ctypes.c_void_p()
+        _check(lib.fpm_init(N, W, q.shape[0], q.ctypes.data_as(_u32p), ctypes.byref(h)))
+        self._h = h
+        self._lib = lib
+        info = FpmInfo()
+        _check(lib.fpm_get_info(h, ctypes.byref(info)))
+        self.info = info
+        self.N, self.W, self.L, self.K = info.N, W, info.L, info.K
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.fpm_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def primes(self) -> np.ndarray:
+        out = np.zeros(self.K, np.uint32)
+        _check(self._lib.fpm_get_primes(self._h, out.ctypes.data_as(_u32p)))
+        return out
+
+    def run(self, a, b, out=None) -> np.ndarray:
+        """c = a b on host arrays (N x L u32)."""
+        a = _limbs(a, self.N, self.L, "a")
+        b = _limbs(b, self.N, self.L, "b")
+        c = np.empty((self.N, self.L), np.uint32) if out is None else out
+        _check(self._lib.fpm_run(self._h, a.ctypes.data, b.ctypes.data, c.ctypes.data))
+        return c
+
+    def run_device(self, d_a: int, d_b: int, d_c: int, stream: int = 0):
+        """c = a b on device pointers (ints), enqueued on a cudaStream_t (int)."""
+        _check(self._lib.fpm_run_device(self._h, d_a, d_b, d_c, stream or None))
+
+    def stage_decompose(self, d_limbs: int, d_res: int, operand: int, stream: int = 0):
+        _check(self._lib.fpm_stage_decompose(self._h, d_limbs, d_res, operand, stream or None))
+
+    def stage_transform(self, d_A: int, d_B: int, mode: int, stream: int = 0):
+        _check(self._lib.fpm_stage_transform(self._h, d_A, d_B, mode, stream or None))
+
+    def stage_crt(self, d_y: int, d_c: int, stream: int = 0):
+        _check(self._lib.fpm_stage_crt(self._h, d_y, d_c, stream or None))
+
+
+# ---------------------------------------------------------------------------
+# The reference's interface (fherma.h:16-48), numpy in place of fherma::Tensor.
+
+@dataclass
+class Point:
+    N: int
+    W: int
+    L: int
+    q: np.ndarray            # L u32
+
+
+@dataclass
+class Inputs:
+    a: np.ndarray            # N x L u32
+    b: np.ndarray
+
+
+@dataclass
+class Outputs:
+    c: np.ndarray = field(default=None)   # N x L u32
+
+
+def fherma_init(p: Point) -> Context:
+    q = np.ascontiguousarray(p.q, dtype=np.uint32).reshape(-1)
+    if q.shape[0] != p.L:
+        raise FpmError(FPM_EINVAL, f"q has {q.shape[0]} limbs, expected L = {p.L}")
+    return Context(p.N, p.W, q)
+
+
+def fherma_run(state: Context, inputs: Inputs) -> Outputs:
+    return Outputs(c=state.run(inputs.a, inputs.b))
+
+
+def fherma_free(state: Context | None):
+    if state is not None:
+        state.close()

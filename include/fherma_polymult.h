@@ -1,0 +1,102 @@
+/*
+ * fherma_polymult.h - C ABI of the B200 exact negacyclic multiplier.
+ *
+ *     c = a * b  mod (X^N + 1, q)
+ *
+ * computed exactly for coefficients of up to 2048 bits, each stored as L
+ * little-endian u32 limbs (L = ceil(W / 32)); operands and result are N x L
+ * arrays, coefficient-major, with every coefficient in [0, q).
+ *
+ * Plain C: opaque handles, pointers and sizes; no C++ or torch types.  Every
+ * function returns 0 on success or one of the FPM_E* codes; the message of the
+ * last failure on the calling thread is in fpm_last_error().  There is no CPU
+ * fallback: without a usable CUDA device, fpm_init fails with FPM_ECUDA.
+ *
+ * The reference (Akram275/fherma-polymult) exposes the same three steps as C++
+ * functions taking std::vector-based structs (fherma.h:46-48).  Those exact C++
+ * symbols are exported too (declared in fherma_abi.h), so the reference's
+ * generated harness links against this library unchanged.
+ */
+#ifndef FHERMA_POLYMULT_H
+#define FHERMA_POLYMULT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FPM_API __attribute__((visibility("default")))
+#else
+#define FPM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FPM_OK 0
+#define FPM_EINVAL 1    /* bad argument or out-of-range point (N, L, q) */
+#define FPM_ECUDA 2     /* CUDA runtime failure */
+#define FPM_ENOMEM 3    /* device or host allocation failed */
+#define FPM_EINTERNAL 4 /* anything else */
+
+typedef struct fpm_ctx fpm_ctx;
+
+typedef struct fpm_info {
+    uint32_t N, W, L;
+    uint32_t K;           /* primes in the RNS basis */
+    uint32_t logN, logR, logS; /* transform geometry: N = 2^logR x 2^logS */
+    int32_t device;       /* CUDA device the context lives on (-1: host-only query) */
+    uint64_t device_bytes; /* device memory the context holds: tables + workspaces */
+} fpm_info;
+
+/* Replaces fherma_init (reference fherma.h:46, solve.cu:710-869): builds the
+ * prime basis and constant tables for (N, q) and keeps them resident on the
+ * current CUDA device.  q has L limbs with a nonzero top limb; N is a power of
+ * two in [2, 2^22]; 1 <= L <= 64.  W is recorded, as the reference does. */
+FPM_API int fpm_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, fpm_ctx** out);
+
+/* Replaces fherma_run (reference fherma.h:47, solve.cu:871-1059): one product
+ * on HOST buffers a, b, c (N x L u32 each, any host memory); returns when c is
+ * written.  Calls on one context must not overlap. */
+FPM_API int fpm_run(fpm_ctx* ctx, const uint32_t* a, const uint32_t* b, uint32_t* c);
+
+/* One product on DEVICE buffers (N x L u32 each), enqueued on `stream` (a
+ * cudaStream_t, NULL for the legacy default stream); returns after enqueueing.
+ * Calls on one context must be ordered on one stream (they share workspaces). */
+FPM_API int fpm_run_device(fpm_ctx* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, void* stream);
+
+/* Replaces fherma_free (reference fherma.h:48, solve.cu:1061-1083); accepts
+ * NULL. */
+FPM_API void fpm_free(fpm_ctx* ctx);
+
+/* Message of the last failure on this thread ("" if none). */
+FPM_API const char* fpm_last_error(void);
+
+FPM_API int fpm_get_info(const fpm_ctx* ctx, fpm_info* out);
+/* Host-only: the plan fpm_init would build for (N, q) (no CUDA call): fills
+ * out (device = -1) and, if primes is not NULL, the K primes.  Used to check a
+ * point and to size its device footprint before admitting it. */
+FPM_API int fpm_plan_info(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, fpm_info* out, uint32_t* primes);
+/* The K primes of the RNS basis, in order (same set and order as the
+ * reference's make_plan, rns_plan.h:138-153). */
+FPM_API int fpm_get_primes(const fpm_ctx* ctx, uint32_t* out);
+
+/* Stage entry points on device buffers, enqueued on `stream` (no reference
+ * counterpart as functions; they expose the reference's kernels' results for
+ * stage-by-stage checks):
+ *   decompose: limbs (N x L) -> residues (K x N, prime-major); operand 0 gives
+ *              a mod p_j, operand 1 gives b mod p_j times the pointwise scale
+ *              N^-1 (P/p_j)^-1 2^32 (reference k_decompose, solve.cu:98-126);
+ *   transform: mode 0: A, B -> y_j = INTT(NTT(A) NTT(B)) in A (reference
+ *              k_ntt_cols / k_ntt_rows_mul, solve.cu:130-233); mode 1: forward
+ *              transforms of A and B in place, bit-reversed order;
+ *   crt:       y (K x N) -> c (N x L) mod q (reference k_crt, solve.cu:264-277). */
+FPM_API int fpm_stage_decompose(fpm_ctx* ctx, const uint32_t* d_limbs, uint32_t* d_res, int operand, void* stream);
+FPM_API int fpm_stage_transform(fpm_ctx* ctx, uint32_t* d_A, uint32_t* d_B, int mode, void* stream);
+FPM_API int fpm_stage_crt(fpm_ctx* ctx, const uint32_t* d_y, uint32_t* d_c, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FHERMA_POLYMULT_H */
