@@ -27,6 +27,9 @@
 struct uint2 {
     uint32_t x, y;
 };
+struct uint4 {
+    uint32_t x, y, z, w;
+};
 #else
 #include <cuda_runtime.h>
 #endif

@@ -1,0 +1,206 @@
+// Decompose on the 5th-generation tensor cores (tcgen05, kind::i8).
+//
+// x mod p_j = sum_k byte_k(x) (2^(8k) mod p_j) mod p_j over the 4L bytes of a
+// coefficient.  Splitting each constant into its 4 bytes turns the sum into an
+// integer GEMM over 8-bit operands:
+//
+//     D[m][4j + s] = sum_k byte_k(x_m) * byte_s(2^(8k) sigma_j mod p_j)
+//     x_m mod p_j  = (sum_s D[m][4j + s] 2^(8s)) mod p_j
+//
+// with sigma_j = 1 for operand a and the pointwise scale for operand b.  Every
+// D entry is below 4L 255^2 < 2^24, so the s32 accumulators are exact and the
+// fold in the epilogue (a 49-bit value reduced mod p_j) is the only modular
+// step.  (Reference: the same sum on CUDA cores, decompose_many rns.cuh:110-128.)
+//
+// Block = 128 coefficients (the MMA's M); the operand tile A (128 x 4L bytes,
+// a contiguous run of the caller's limbs) is staged once in shared memory in
+// the canonical K-major layout; the constant matrix B streams in chunks of 32
+// primes (128 GEMM columns, a prebuilt image, one bulk copy each) through two
+// shared-memory slots, and D alternates between two 128-column TMEM buffers,
+// so the MMAs of chunk c + 1 overlap the epilogue of chunk c.
+//   warp 0      : TMEM allocation, B copies, MMA issue (one thread)
+//   warps 1 - 4 : epilogue, one thread per TMEM lane (= coefficient): tcgen05.ld,
+//                 fold, coalesced stores of each prime's 128 residues.
+#include "device.cuh"
+#include "kernels.h"
+#include "tc.cuh"
+
+namespace fpm {
+
+namespace {
+
+constexpr int kThreads = 160;
+constexpr uint32_t kRows = 128;
+constexpr uint32_t kCols = 128;                    // GEMM columns per chunk (32 primes)
+constexpr uint32_t kALbo = kRows * 16 + 16;        // A: K-adjacent core matrices, padded
+                                                   // so a warp's 32 word stores hit 32 banks
+
+struct Smem {
+    uint8_t* a;
+    uint8_t* b[2];
+    uint64_t* full;        // [2] B chunk landed
+    uint64_t* mma_done;    // [2] MMAs of the chunk finished (D ready, B slot free)
+    uint64_t* tmem_empty;  // [2] epilogue finished reading the D buffer
+    uint32_t* tmem_base;
+};
+
+__host__ __device__ inline uint32_t a_bytes(uint32_t kb) { return (kb / 16) * kALbo; }
+
+__device__ inline Smem carve(uint8_t* base, uint32_t kb) {
+    Smem s;
+    s.a = base;
+    s.b[0] = base + ((a_bytes(kb) + 127) & ~127u);
+    s.b[1] = s.b[0] + kCols * kb;
+    s.full = reinterpret_cast<uint64_t*>(s.b[1] + kCols * kb);
+    s.mma_done = s.full + 2;
+    s.tmem_empty = s.full + 4;
+    s.tmem_base = reinterpret_cast<uint32_t*>(s.full + 6);
+    return s;
+}
+
+// (lo + hi 2^32) mod p for the 49-bit epilogue sums: f = {p, 2^32 mod p, its
+// Shoup companion, floor(2^32 / p)}.
+__device__ __forceinline__ uint32_t fold49(uint64_t v, uint4 f) {
+    const uint32_t lo = shoup(static_cast<uint32_t>(v), 1u, f.w, f.x);
+    const uint32_t hi = shoup(static_cast<uint32_t>(v >> 32), f.y, f.z, f.x);
+    return add_mod(lo, hi, f.x);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_decompose_tc(DevPoint d, const uint32_t* __restrict__ limbs, uint32_t* __restrict__ res, int operand) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    const uint32_t kb = d.dec_kb;          // GEMM K in bytes (4L rounded up to 32)
+    const int nch = d.dec_chunks;
+    const Smem sm = carve(smem_raw, kb);
+    const uint8_t* img = operand ? d.dec_img_b : d.dec_img_a;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t n0 = blockIdx.x * kRows;
+    const uint32_t nk = min(kRows, d.N - n0);
+    const int L = d.L;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 2; ++i) {
+            tc::mbar_init(&sm.full[i], 1);
+            tc::mbar_init(&sm.mma_done[i], 1);
+            tc::mbar_init(&sm.tmem_empty[i], kRows);
+        }
+        tc::fence_mbar_init();
+    }
+    if (warp == 0) tc::tmem_alloc(sm.tmem_base, 2 * kCols);
+
+    // Operand tile: word l of row m -> core matrix (l / 4) along K, row m.
+    {
+        const uint32_t kw = kb / 4;
+        const uint32_t* src = limbs + static_cast<size_t>(n0) * L;
+        for (uint32_t w = threadIdx.x; w < kRows * kw; w += kThreads) {
+            const uint32_t m = w / kw, l = w - m * kw;
+            const uint32_t v = (m < nk && l < static_cast<uint32_t>(L)) ? src[m * L + l] : 0u;
+            *reinterpret_cast<uint32_t*>(sm.a + (l >> 2) * kALbo + m * 16 + (l & 3) * 4) = v;
+        }
+    }
+    tc::fence_proxy_async_smem();
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *sm.tmem_base;
+    bool ok = true;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            const uint32_t chunk_bytes = kCols * kb;
+            const int pre = nch < 2 ? nch : 2;
+            for (int c = 0; c < pre; ++c) {
+                tc::mbar_arrive_expect_tx(&sm.full[c], chunk_bytes);
+                tc::bulk_g2s(sm.b[c], img + static_cast<size_t>(c) * chunk_bytes, chunk_bytes, &sm.full[c]);
+            }
+            const uint32_t idesc = tc::idesc_u8(kCols);
+            const uint32_t a0 = tc::smem_addr(sm.a);
+            for (int c = 0; c < nch && ok; ++c) {
+                const int s = c & 1;
+                ok = tc::wait_parity(&sm.full[s], (c >> 1) & 1);
+                if (ok && c >= 2) ok = tc::wait_parity(&sm.tmem_empty[s], ((c - 2) >> 1) & 1);
+                if (!ok) break;
+                tc::tc_fence_after();
+                const uint32_t b0 = tc::smem_addr(sm.b[s]);
+                for (uint32_t kk = 0; kk < kb / 32; ++kk) {
+                    const uint64_t ad = tc::smem_desc(a0 + kk * 2 * kALbo, kALbo, 128);
+                    const uint64_t bd = tc::smem_desc(b0 + kk * 2 * (kCols * 16), kCols * 16, 128);
+                    tc::mma_u8(tmem + s * kCols, ad, bd, idesc, kk > 0);
+                }
+                tc::mma_commit(&sm.mma_done[s]);
+                if (c >= 1 && c + 1 < nch) {
+                    const int s1 = (c - 1) & 1;
+                    ok = tc::wait_parity(&sm.mma_done[s1], ((c - 1) >> 1) & 1);
+                    if (!ok) break;
+                    tc::mbar_arrive_expect_tx(&sm.full[s1], chunk_bytes);
+                    tc::bulk_g2s(sm.b[s1], img + static_cast<size_t>(c + 1) * chunk_bytes, chunk_bytes,
+                                 &sm.full[s1]);
+                }
+            }
+            if (ok) {
+                // The last MMAs must finish before the block can release TMEM.
+                const int c = nch - 1;
+                ok = tc::wait_parity(&sm.mma_done[c & 1], (c >> 1) & 1);
+            }
+        }
+        __syncwarp();
+    } else {
+        const uint32_t q = warp & 3;                   // TMEM lane quadrant of this warp
+        const uint32_t m = q * 32 + lane;
+        const uint32_t tq = tmem + ((q * 32) << 16);
+        for (int c = 0; c < nch; ++c) {
+            const int s = c & 1;
+            ok = tc::wait_parity(&sm.mma_done[s], (c >> 1) & 1);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) break;
+            tc::tc_fence_after();
+#pragma unroll 1
+            for (int piece = 0; piece < 4; ++piece) {
+                uint32_t r[32];
+                tc::tmem_ld32(tq + s * kCols + piece * 32, r);
+                tc::tmem_ld_wait();
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const int j = c * 32 + piece * 8 + i;
+                    if (j < d.K && m < nk) {
+                        const uint64_t v = static_cast<uint64_t>(r[4 * i]) + (static_cast<uint64_t>(r[4 * i + 1]) << 8) +
+                                           (static_cast<uint64_t>(r[4 * i + 2]) << 16) +
+                                           (static_cast<uint64_t>(r[4 * i + 3]) << 24);
+                        res[static_cast<size_t>(j) * d.N + n0 + m] = fold49(v, d.dec_fold[j]);
+                    }
+                }
+            }
+            tc::tc_fence_before();
+            tc::mbar_arrive(&sm.tmem_empty[s]);
+        }
+    }
+
+    if (!ok) atomicOr(d.err, 1u);
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, 2 * kCols);
+    }
+}
+
+// At least 78 KB, so no more than two blocks (2 x 256 TMEM columns) share an SM.
+size_t smem_bytes(uint32_t kb) {
+    const size_t need = ((a_bytes(kb) + 127) & ~127u) + 2 * kCols * kb + 8 * sizeof(uint64_t);
+    return need > 78 * 1024 ? need : 78 * 1024;
+}
+
+}  // namespace
+
+void decompose_tc_init_attributes() {
+    check(cudaFuncSetAttribute(k_decompose_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(smem_bytes(4 * kMaxL))),
+          "decompose_tc smem");
+}
+
+void launch_decompose_tc(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, cudaStream_t st) {
+    const uint32_t blocks = (d.N + kRows - 1) / kRows;
+    k_decompose_tc<<<blocks, kThreads, smem_bytes(d.dec_kb), st>>>(d, limbs, res, operand);
+}
+
+}  // namespace fpm

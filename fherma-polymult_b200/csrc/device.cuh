@@ -28,6 +28,18 @@ struct DevPoint {
     const uint32_t* M;         // K x L
     const uint32_t* negvP;     // (K + 1) x L
     const double* p_recip;     // K
+    // tensor-core decompose
+    uint32_t dec_kb;
+    int dec_chunks;
+    const uint8_t* dec_img_a;
+    const uint8_t* dec_img_b;
+    const uint4* dec_fold;     // K
+    // tensor-core CRT
+    uint32_t crt_u;
+    uint32_t crt_tmem_cols;
+    const uint8_t* crt_img;
+    // error word: bit 0 decompose, bit 1 CRT (a pipeline wait timed out)
+    uint32_t* err;
 };
 
 // What the row kernel does with its tile.

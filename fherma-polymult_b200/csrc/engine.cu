@@ -8,6 +8,7 @@
 #include "engine.h"
 #include "kernels.h"
 
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <stdexcept>
@@ -24,6 +25,8 @@ void ensure_kernel_attributes(int device) {
     ntt_init_attributes();
     decompose_init_attributes();
     crt_init_attributes();
+    decompose_tc_init_attributes();
+    crt_tc_init_attributes();
     done.push_back(device);
 }
 
@@ -71,6 +74,17 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
         dp_.M = upload(pl.M);
         dp_.negvP = upload(pl.negvP);
         dp_.p_recip = upload(pl.p_recip);
+        dp_.dec_kb = pl.dec_kb;
+        dp_.dec_chunks = static_cast<int>(pl.dec_chunks);
+        dp_.dec_img_a = upload(pl.dec_img_a);
+        dp_.dec_img_b = upload(pl.dec_img_b);
+        dp_.dec_fold = upload(pl.dec_fold);
+        dp_.crt_u = pl.crt_u;
+        dp_.crt_tmem_cols = pl.crt_tmem_cols;
+        dp_.crt_img = upload(pl.crt_img);
+        dp_.err = dalloc<uint32_t>(1);
+        check(cudaMemset(dp_.err, 0, sizeof(uint32_t)), "memset");
+        if (const char* k = std::getenv("FPM_KERNELS")) simt_ = std::strcmp(k, "simt") == 0;
         A_ = dalloc<uint32_t>(residues());
         B_ = dalloc<uint32_t>(residues());
         check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
@@ -99,8 +113,31 @@ void Engine::release() {
     ha_ = hb_ = hc_ = nullptr;
 }
 
+void Engine::launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, cudaStream_t st) {
+    if (simt_) {
+        launch_decompose(dp_, d_limbs, d_res, operand, st);
+    } else {
+        launch_decompose_tc(dp_, d_limbs, d_res, operand, st);
+    }
+}
+
+void Engine::launch_crt_any(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st) {
+    if (simt_ || !crt_uses_tc(plan_)) {
+        launch_crt(dp_, d_y, d_c, st);
+    } else {
+        launch_crt_tc(dp_, d_y, d_c, st);
+    }
+}
+
+uint32_t Engine::take_error() {
+    uint32_t e = 0;
+    check(cudaMemcpy(&e, dp_.err, sizeof(e), cudaMemcpyDeviceToHost), "read error word");
+    if (e) check(cudaMemset(dp_.err, 0, sizeof(e)), "clear error word");
+    return e;
+}
+
 void Engine::decompose(const uint32_t* d_limbs, uint32_t* d_res, int operand, cudaStream_t st) {
-    launch_decompose(dp_, d_limbs, d_res, operand, st);
+    launch_dec(d_limbs, d_res, operand, st);
     check(cudaGetLastError(), "decompose launch");
 }
 
@@ -110,15 +147,15 @@ void Engine::transform(uint32_t* d_A, uint32_t* d_B, int mode, cudaStream_t st) 
 }
 
 void Engine::crt(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st) {
-    launch_crt(dp_, d_y, d_c, st);
+    launch_crt_any(d_y, d_c, st);
     check(cudaGetLastError(), "crt launch");
 }
 
 void Engine::run_device(const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t st) {
-    launch_decompose(dp_, d_a, A_, 0, st);
-    launch_decompose(dp_, d_b, B_, 1, st);
+    launch_dec(d_a, A_, 0, st);
+    launch_dec(d_b, B_, 1, st);
     launch_ntt(dp_, A_, B_, kRowProduct, st);
-    launch_crt(dp_, A_, d_c, st);
+    launch_crt_any(A_, d_c, st);
     check(cudaGetLastError(), "product launch");
 }
 
@@ -139,6 +176,9 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
     run_device(la_, lb_, lc_, stream_);
     check(cudaMemcpyAsync(hc_, lc_, bytes, cudaMemcpyDeviceToHost, stream_), "copy c");
     check(cudaStreamSynchronize(stream_), "product");
+    if (const uint32_t e = take_error()) {
+        throw std::runtime_error("a kernel pipeline wait timed out (error word " + std::to_string(e) + ")");
+    }
     std::memcpy(c, hc_, bytes);
 }
 

@@ -37,11 +37,17 @@ public:
     void transform(uint32_t* d_A, uint32_t* d_B, int mode, cudaStream_t st);
     void crt(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st);
 
+    // Reads and clears the device error word (nonzero: a pipeline wait in a
+    // tensor-core kernel timed out); synchronous.
+    uint32_t take_error();
+
     size_t words() const { return static_cast<size_t>(plan_.N) * plan_.L; }
     size_t residues() const { return static_cast<size_t>(plan_.K) * plan_.N; }
 
 private:
     void release();
+    void launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, cudaStream_t st);
+    void launch_crt_any(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st);
     template <class T>
     T* dalloc(size_t count);
     template <class T>
@@ -50,6 +56,7 @@ private:
     HostPlan plan_;
     DevPoint dp_{};
     int device_ = 0;
+    bool simt_ = false;        // FPM_KERNELS=simt: CUDA-core decompose and CRT
     std::vector<void*> dmem_;
     uint32_t* A_ = nullptr;   // K x N residues
     uint32_t* B_ = nullptr;

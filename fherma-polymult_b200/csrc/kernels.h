@@ -34,6 +34,8 @@ size_t row_smem();
 void ntt_init_attributes();
 void decompose_init_attributes();
 void crt_init_attributes();
+void decompose_tc_init_attributes();
+void crt_tc_init_attributes();
 
 // limbs (N x L, coefficient-major) -> residues (K x N); operand 1 (b) is
 // scaled for the pointwise step.
@@ -43,7 +45,11 @@ void launch_decompose(const DevPoint& d, const uint32_t* limbs, uint32_t* res, i
 // both in place (mode kRowForward).
 void launch_ntt(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStream_t st);
 
-// y_j (K x N) -> c (N x L) mod q.
+// The same on the tensor cores.
+void launch_decompose_tc(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, cudaStream_t st);
+
+// y_j (K x N) -> c (N x L) mod q: CUDA cores, and tensor cores (L >= 2).
 void launch_crt(const DevPoint& d, const uint32_t* Y, uint32_t* c, cudaStream_t st);
+void launch_crt_tc(const DevPoint& d, const uint32_t* Y, uint32_t* c, cudaStream_t st);
 
 }  // namespace fpm

@@ -96,7 +96,8 @@ size_t device_footprint(const HostPlan& pl) {
     size_t t = bytes(pl.pc) + bytes(pl.dec_a) + bytes(pl.dec_b) + bytes(pl.col_f) + bytes(pl.col_i) +
                bytes(pl.row_u_f) + bytes(pl.row_u_i) + bytes(pl.row_q_f) + bytes(pl.row_q_i) +
                bytes(pl.full_f) + bytes(pl.full_i) + bytes(pl.q) + bytes(pl.M) + bytes(pl.negvP) +
-               bytes(pl.p_recip);
+               bytes(pl.p_recip) + bytes(pl.dec_img_a) + bytes(pl.dec_img_b) + bytes(pl.dec_fold) +
+               bytes(pl.crt_img) + sizeof(uint32_t);
     t += 2 * static_cast<size_t>(pl.K) * pl.N * sizeof(uint32_t);   // residue workspaces
     t += 3 * static_cast<size_t>(pl.N) * pl.L * sizeof(uint32_t);   // host-path limb buffers
     return t;
@@ -237,6 +238,31 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
         }
     }
 
+    // Tensor-core decompose images and fold constants.
+    pl.dec_kb = (4 * static_cast<uint32_t>(L) + 31) / 32 * 32;
+    pl.dec_chunks = static_cast<uint32_t>((K + 31) / 32);
+    const size_t dchunk = static_cast<size_t>(128) * pl.dec_kb;
+    pl.dec_img_a.assign(dchunk * pl.dec_chunks, 0);
+    pl.dec_img_b.assign(dchunk * pl.dec_chunks, 0);
+    pl.dec_fold.resize(K);
+    for (int j = 0; j < K; ++j) {
+        const uint32_t p = pl.primes[j];
+        const uint32_t r32 = static_cast<uint32_t>((1ull << 32) % p);
+        pl.dec_fold[j] = uint4{p, r32, shoup_of(r32, p), static_cast<uint32_t>((1ull << 32) / p)};
+        const uint32_t scale_b = pl.dec_b[static_cast<size_t>(j) * L].x;   // 2^0 * scale
+        const size_t chunk = static_cast<size_t>(j / 32) * dchunk;
+        for (int s = 0; s < 4; ++s) {
+            const uint32_t col = 4 * (j % 32) + s;
+            for (uint32_t k = 0; k < 4 * static_cast<uint32_t>(L); ++k) {
+                const uint32_t ca = pow_mod(2, 8ull * k, p);
+                const uint32_t cb = static_cast<uint32_t>(static_cast<uint64_t>(ca) * scale_b % p);
+                const size_t at = chunk + (k / 16) * (128 * 16) + col * 16 + (k % 16);
+                pl.dec_img_a[at] = static_cast<uint8_t>(ca >> (8 * s));
+                pl.dec_img_b[at] = static_cast<uint8_t>(cb >> (8 * s));
+            }
+        }
+    }
+
     // M_j = prod_{i != j} p_i mod q, P mod q, and negvP_v = (q - v P mod q) mod q
     // for v = 0..K (reference rns_plan.h:224-247).
     pl.M.assign(static_cast<size_t>(K) * L, 0);
@@ -259,6 +285,29 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
         std::vector<uint32_t> neg = pl.q;
         limbs_sub(neg.data(), L, t.data(), L);
         std::copy(neg.begin(), neg.end(), pl.negvP.begin() + static_cast<size_t>(v) * L);
+    }
+
+    // Tensor-core CRT image.
+    if (crt_uses_tc(pl)) {
+        pl.crt_u = (4 * static_cast<uint32_t>(L) - 1 + 31) / 32 * 32;
+        pl.crt_tmem_cols = 32;
+        while (pl.crt_tmem_cols < pl.crt_u) pl.crt_tmem_cols *= 2;
+        const uint32_t chunks = static_cast<uint32_t>((K + 31) / 32);
+        const size_t cchunk = static_cast<size_t>(pl.crt_u) * 128;
+        const uint32_t low_bytes = 4 * static_cast<uint32_t>(L - 1);
+        pl.crt_img.assign(cchunk * chunks, 0);
+        for (int j = 0; j < K; ++j) {
+            const uint32_t* m = &pl.M[static_cast<size_t>(j) * L];
+            for (int s = 0; s < 4; ++s) {
+                const uint32_t kbyte = 4 * (j % 32) + s;   // K index within the chunk
+                for (uint32_t u = s; u < pl.crt_u && u - s < low_bytes; ++u) {
+                    const uint32_t byte = u - s;
+                    const size_t at = static_cast<size_t>(j / 32) * cchunk + (kbyte / 16) * (pl.crt_u * 16) +
+                                      u * 16 + (kbyte % 16);
+                    pl.crt_img[at] = static_cast<uint8_t>(m[byte / 4] >> (8 * (byte % 4)));
+                }
+            }
+        }
     }
     return pl;
 }

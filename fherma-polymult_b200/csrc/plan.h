@@ -67,7 +67,28 @@ struct HostPlan {
     // 1 / p_j (K).
     std::vector<uint32_t> M, negvP;
     std::vector<double> p_recip;
+
+    // Tensor-core decompose (decompose_tc.cu): the GEMM's B operand, the bytes of
+    // c_{j,k} = 2^(8k) sigma_j mod p_j (k < 4L) split per byte s into GEMM column
+    // 4j + s, in chunks of 32 primes (128 columns), each chunk a ready-made
+    // shared-memory image in the UMMA K-major no-swizzle layout
+    // [dec_kb / 16 core columns][128 rows][16 bytes].  One image per operand.
+    uint32_t dec_kb = 0;                     // GEMM K in bytes: 4L rounded up to 32
+    uint32_t dec_chunks = 0;                 // ceil(K / 32)
+    std::vector<uint8_t> dec_img_a, dec_img_b;
+    std::vector<uint4> dec_fold;             // K: {p, 2^32 mod p, its Shoup companion, floor(2^32 / p)}
+
+    // Tensor-core CRT (crt_tc.cu), L >= 2: B operand, row u (a byte position of
+    // X_low = sum_j y_j M_j[0 .. L-2]) and column 4j + s hold byte (u - s) of
+    // M_j's low L - 1 limbs; u < crt_u = 4L - 1 rounded up to 32.  Chunks of 32
+    // primes (128 K bytes), image [8 core columns][crt_u rows][16 bytes].
+    uint32_t crt_u = 0;
+    uint32_t crt_tmem_cols = 0;              // power of two >= crt_u
+    std::vector<uint8_t> crt_img;
 };
+
+// Which CRT kernel the point uses: the tensor-core one needs L >= 2.
+inline bool crt_uses_tc(const HostPlan& pl) { return pl.L >= 2; }
 
 // Device bytes an Engine for this plan holds (tables, residue workspaces and
 // the limb buffers of the host path).
