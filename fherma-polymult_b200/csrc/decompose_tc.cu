@@ -19,8 +19,9 @@
 // shared-memory slots, and D alternates between two 128-column TMEM buffers,
 // so the MMAs of chunk c + 1 overlap the epilogue of chunk c.
 //   warp 0      : TMEM allocation, B copies, MMA issue (one thread)
-//   warps 1 - 4 : epilogue, one thread per TMEM lane (= coefficient): tcgen05.ld,
-//                 fold, coalesced stores of each prime's 128 residues.
+//   warps 1 - 8 : epilogue, two warps per TMEM lane quadrant (each takes half of
+//                 a chunk's 32 primes), one thread per lane (= coefficient):
+//                 tcgen05.ld, fold, coalesced stores of each prime's residues.
 #include "device.cuh"
 #include "kernels.h"
 #include "tc.cuh"
@@ -29,7 +30,8 @@ namespace fpm {
 
 namespace {
 
-constexpr int kThreads = 160;
+constexpr int kThreads = 288;                      // warp 0 + 8 epilogue warps
+constexpr uint32_t kEpi = 256;                     // epilogue threads
 constexpr uint32_t kRows = 128;
 constexpr uint32_t kCols = 128;                    // GEMM columns per chunk (32 primes)
 constexpr uint32_t kALbo = kRows * 16 + 16;        // A: K-adjacent core matrices, padded
@@ -37,11 +39,12 @@ constexpr uint32_t kALbo = kRows * 16 + 16;        // A: K-adjacent core matrice
 
 struct Smem {
     uint8_t* a;
-    uint8_t* b[2];
+    uint8_t* b0;           // B slot s at b0 + s * kCols * kb
     uint64_t* full;        // [2] B chunk landed
     uint64_t* mma_done;    // [2] MMAs of the chunk finished (D ready, B slot free)
     uint64_t* tmem_empty;  // [2] epilogue finished reading the D buffer
     uint32_t* tmem_base;
+    uint4* fold;           // [kMaxK] fold constants, staged once per block
 };
 
 __host__ __device__ inline uint32_t a_bytes(uint32_t kb) { return (kb / 16) * kALbo; }
@@ -49,12 +52,12 @@ __host__ __device__ inline uint32_t a_bytes(uint32_t kb) { return (kb / 16) * kA
 __device__ inline Smem carve(uint8_t* base, uint32_t kb) {
     Smem s;
     s.a = base;
-    s.b[0] = base + ((a_bytes(kb) + 127) & ~127u);
-    s.b[1] = s.b[0] + kCols * kb;
-    s.full = reinterpret_cast<uint64_t*>(s.b[1] + kCols * kb);
+    s.b0 = base + ((a_bytes(kb) + 127) & ~127u);
+    s.full = reinterpret_cast<uint64_t*>(s.b0 + 2 * kCols * kb);
     s.mma_done = s.full + 2;
     s.tmem_empty = s.full + 4;
     s.tmem_base = reinterpret_cast<uint32_t*>(s.full + 6);
+    s.fold = reinterpret_cast<uint4*>(s.full + 8);
     return s;
 }
 
@@ -82,21 +85,58 @@ __global__ void __launch_bounds__(kThreads)
         for (int i = 0; i < 2; ++i) {
             tc::mbar_init(&sm.full[i], 1);
             tc::mbar_init(&sm.mma_done[i], 1);
-            tc::mbar_init(&sm.tmem_empty[i], kRows);
+            tc::mbar_init(&sm.tmem_empty[i], kEpi);
         }
         tc::fence_mbar_init();
     }
     if (warp == 0) tc::tmem_alloc(sm.tmem_base, 2 * kCols);
+    for (int j = threadIdx.x; j < d.K; j += kThreads) sm.fold[j] = d.dec_fold[j];
 
-    // Operand tile: word l of row m -> core matrix (l / 4) along K, row m.
+    // Operand tile: word l of row m goes to core matrix l / 4 along K, row m.
+    // The block's nk L words are contiguous and 16-byte aligned (n0 L 4 = 512 L
+    // bytes), so they are read as 16-byte chunks, 8 in flight per thread.
     {
         const uint32_t kw = kb / 4;
-        const uint32_t* src = limbs + static_cast<size_t>(n0) * L;
-        for (uint32_t w = threadIdx.x; w < kRows * kw; w += kThreads) {
-            const uint32_t m = w / kw, l = w - m * kw;
-            const uint32_t v = (m < nk && l < static_cast<uint32_t>(L)) ? src[m * L + l] : 0u;
-            *reinterpret_cast<uint32_t*>(sm.a + (l >> 2) * kALbo + m * 16 + (l & 3) * 4) = v;
+        if (kw != static_cast<uint32_t>(L) || nk < kRows) {
+            // Zero padding: rows past nk and words past L.
+            for (uint32_t i = threadIdx.x; i < a_bytes(kb) / 16; i += kThreads)
+                reinterpret_cast<uint4*>(sm.a)[i] = make_uint4(0, 0, 0, 0);
+            __syncthreads();
         }
+        const uint32_t total = nk * static_cast<uint32_t>(L);
+        const uint32_t n16 = total / 4;
+        const uint4* src4 = reinterpret_cast<const uint4*>(limbs + static_cast<size_t>(n0) * L);
+        // w / L = mulhi(w, ceil(2^32 / L)) exactly for w < 2^16 (L = 1 divides trivially).
+        const uint32_t inv_l = L == 1 ? 0u : 0xFFFFFFFFu / static_cast<uint32_t>(L) + 1;
+        auto row_of = [&](uint32_t w) { return L == 1 ? w : __umulhi(w, inv_l); };
+        auto place = [&](uint32_t w, uint32_t v) {
+            const uint32_t m = row_of(w), l = w - m * L;
+            *reinterpret_cast<uint32_t*>(sm.a + (l >> 2) * kALbo + m * 16 + (l & 3) * 4) = v;
+        };
+        for (uint32_t i0 = threadIdx.x; i0 < n16; i0 += 8 * kThreads) {
+            uint4 v[8];
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                const uint32_t i = i0 + b * kThreads;
+                v[b] = i < n16 ? __ldg(src4 + i) : make_uint4(0, 0, 0, 0);
+            }
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                const uint32_t i = i0 + b * kThreads;
+                if (i >= n16) continue;
+                if ((L & 3) == 0) {
+                    const uint32_t w = 4 * i, m = row_of(w), l = w - m * L;
+                    *reinterpret_cast<uint4*>(sm.a + (l >> 2) * kALbo + m * 16) = v[b];
+                } else {
+                    place(4 * i, v[b].x);
+                    place(4 * i + 1, v[b].y);
+                    place(4 * i + 2, v[b].z);
+                    place(4 * i + 3, v[b].w);
+                }
+            }
+        }
+        const uint32_t* src = limbs + static_cast<size_t>(n0) * L;
+        if (threadIdx.x < total - 4 * n16) place(4 * n16 + threadIdx.x, src[4 * n16 + threadIdx.x]);
     }
     tc::fence_proxy_async_smem();
     tc::tc_fence_before();
@@ -111,7 +151,7 @@ __global__ void __launch_bounds__(kThreads)
             const int pre = nch < 2 ? nch : 2;
             for (int c = 0; c < pre; ++c) {
                 tc::mbar_arrive_expect_tx(&sm.full[c], chunk_bytes);
-                tc::bulk_g2s(sm.b[c], img + static_cast<size_t>(c) * chunk_bytes, chunk_bytes, &sm.full[c]);
+                tc::bulk_g2s(sm.b0 + c * chunk_bytes, img + static_cast<size_t>(c) * chunk_bytes, chunk_bytes, &sm.full[c]);
             }
             const uint32_t idesc = tc::idesc_u8(kCols);
             const uint32_t a0 = tc::smem_addr(sm.a);
@@ -121,7 +161,7 @@ __global__ void __launch_bounds__(kThreads)
                 if (ok && c >= 2) ok = tc::wait_parity(&sm.tmem_empty[s], ((c - 2) >> 1) & 1);
                 if (!ok) break;
                 tc::tc_fence_after();
-                const uint32_t b0 = tc::smem_addr(sm.b[s]);
+                const uint32_t b0 = tc::smem_addr(sm.b0 + s * chunk_bytes);
                 for (uint32_t kk = 0; kk < kb / 32; ++kk) {
                     const uint64_t ad = tc::smem_desc(a0 + kk * 2 * kALbo, kALbo, 128);
                     const uint64_t bd = tc::smem_desc(b0 + kk * 2 * (kCols * 16), kCols * 16, 128);
@@ -133,7 +173,7 @@ __global__ void __launch_bounds__(kThreads)
                     ok = tc::wait_parity(&sm.mma_done[s1], ((c - 1) >> 1) & 1);
                     if (!ok) break;
                     tc::mbar_arrive_expect_tx(&sm.full[s1], chunk_bytes);
-                    tc::bulk_g2s(sm.b[s1], img + static_cast<size_t>(c + 1) * chunk_bytes, chunk_bytes,
+                    tc::bulk_g2s(sm.b0 + s1 * chunk_bytes, img + static_cast<size_t>(c + 1) * chunk_bytes, chunk_bytes,
                                  &sm.full[s1]);
                 }
             }
@@ -146,6 +186,7 @@ __global__ void __launch_bounds__(kThreads)
         __syncwarp();
     } else {
         const uint32_t q = warp & 3;                   // TMEM lane quadrant of this warp
+        const int half = (warp - 1) >> 2;              // which 16 primes of each chunk
         const uint32_t m = q * 32 + lane;
         const uint32_t tq = tmem + ((q * 32) << 16);
         for (int c = 0; c < nch; ++c) {
@@ -155,19 +196,26 @@ __global__ void __launch_bounds__(kThreads)
             if (!ok) break;
             tc::tc_fence_after();
 #pragma unroll 1
-            for (int piece = 0; piece < 4; ++piece) {
+            for (int piece = 2 * half; piece < 2 * half + 2; ++piece) {
+                const int j0 = c * 32 + piece * 8;
+                uint4 f[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) f[i] = sm.fold[min(j0 + i, d.K - 1)];
                 uint32_t r[32];
                 tc::tmem_ld32(tq + s * kCols + piece * 32, r);
                 tc::tmem_ld_wait();
+                uint32_t out[8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
-                    const int j = c * 32 + piece * 8 + i;
-                    if (j < d.K && m < nk) {
-                        const uint64_t v = static_cast<uint64_t>(r[4 * i]) + (static_cast<uint64_t>(r[4 * i + 1]) << 8) +
-                                           (static_cast<uint64_t>(r[4 * i + 2]) << 16) +
-                                           (static_cast<uint64_t>(r[4 * i + 3]) << 24);
-                        res[static_cast<size_t>(j) * d.N + n0 + m] = fold49(v, d.dec_fold[j]);
-                    }
+                    const uint64_t v = static_cast<uint64_t>(r[4 * i]) + (static_cast<uint64_t>(r[4 * i + 1]) << 8) +
+                                       (static_cast<uint64_t>(r[4 * i + 2]) << 16) +
+                                       (static_cast<uint64_t>(r[4 * i + 3]) << 24);
+                    out[i] = fold49(v, f[i]);
+                }
+                if (m < nk) {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        if (j0 + i < d.K) res[static_cast<size_t>(j0 + i) * d.N + n0 + m] = out[i];
                 }
             }
             tc::tc_fence_before();
@@ -186,7 +234,7 @@ __global__ void __launch_bounds__(kThreads)
 
 // At least 78 KB, so no more than two blocks (2 x 256 TMEM columns) share an SM.
 size_t smem_bytes(uint32_t kb) {
-    const size_t need = ((a_bytes(kb) + 127) & ~127u) + 2 * kCols * kb + 8 * sizeof(uint64_t);
+    const size_t need = ((a_bytes(kb) + 127) & ~127u) + 2 * kCols * kb + 8 * sizeof(uint64_t) + kMaxK * sizeof(uint4);
     return need > 78 * 1024 ? need : 78 * 1024;
 }
 
