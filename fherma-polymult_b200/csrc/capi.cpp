@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdlib>
 #include <exception>
 #include <new>
 #include <stdexcept>
@@ -46,6 +47,25 @@ int guarded(F&& f) {
 
 cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
 
+int resolve_prime_bits(int prime_bits) {
+    if (prime_bits) return prime_bits;
+    if (const char* v = std::getenv("FPM_PRIME_BITS")) return std::atoi(v);
+    return fpm::kDefaultPrimeBits;
+}
+
+void fill_info(const fpm::HostPlan& pl, uint32_t W, int device, fpm_info* out) {
+    out->N = pl.N;
+    out->W = W;
+    out->L = static_cast<uint32_t>(pl.L);
+    out->K = static_cast<uint32_t>(pl.K);
+    out->logN = pl.g.logN;
+    out->logR = pl.g.logR;
+    out->logS = pl.g.logS;
+    out->device = device;
+    out->device_bytes = fpm::device_footprint(pl);
+    out->prime_bits = static_cast<uint32_t>(pl.pmax_log2);
+}
+
 }  // namespace
 
 extern "C" {
@@ -53,6 +73,10 @@ extern "C" {
 const char* fpm_last_error(void) { return g_error.c_str(); }
 
 int fpm_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, fpm_ctx** out) {
+    return fpm_init_ex(N, W, L, q, 0, out);
+}
+
+int fpm_init_ex(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int prime_bits, fpm_ctx** out) {
     if (!out) return fail(FPM_EINVAL, "fpm_init: out is NULL");
     *out = nullptr;
     if (!q) return fail(FPM_EINVAL, "fpm_init: q is NULL");
@@ -64,7 +88,9 @@ int fpm_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, fpm_ctx** ou
         return fail(FPM_ECUDA, "no CUDA device: this library has no CPU fallback");
     }
     fpm::Engine* e = nullptr;
-    const int rc = guarded([&] { e = new fpm::Engine(N, W, q, static_cast<int>(L)); });
+    const int bits = resolve_prime_bits(prime_bits);
+    if (bits != 30 && bits != 31) return fail(FPM_EINVAL, "prime_bits must be 30 or 31");
+    const int rc = guarded([&] { e = new fpm::Engine(N, W, q, static_cast<int>(L), bits); });
     if (rc) return rc;
     *out = new fpm_ctx{e, W};
     return FPM_OK;
@@ -88,32 +114,22 @@ void fpm_free(fpm_ctx* ctx) {
 
 int fpm_get_info(const fpm_ctx* ctx, fpm_info* out) {
     if (!ctx || !out) return fail(FPM_EINVAL, "fpm_get_info: NULL argument");
-    const fpm::HostPlan& pl = ctx->engine->plan();
-    out->N = pl.N;
-    out->W = ctx->W;
-    out->L = static_cast<uint32_t>(pl.L);
-    out->K = static_cast<uint32_t>(pl.K);
-    out->logN = pl.g.logN;
-    out->logR = pl.g.logR;
-    out->logS = pl.g.logS;
-    out->device = ctx->engine->device();
-    out->device_bytes = fpm::device_footprint(pl);
+    fill_info(ctx->engine->plan(), ctx->W, ctx->engine->device(), out);
     return FPM_OK;
 }
 
 int fpm_plan_info(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, fpm_info* out, uint32_t* primes) {
+    return fpm_plan_info_ex(N, W, L, q, 0, out, primes);
+}
+
+int fpm_plan_info_ex(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int prime_bits, fpm_info* out,
+                     uint32_t* primes) {
     if (!q || !out) return fail(FPM_EINVAL, "fpm_plan_info: NULL argument");
+    const int bits = resolve_prime_bits(prime_bits);
+    if (bits != 30 && bits != 31) return fail(FPM_EINVAL, "prime_bits must be 30 or 31");
     return guarded([&] {
-        const fpm::HostPlan pl = fpm::make_plan(N, W, q, static_cast<int>(L));
-        out->N = pl.N;
-        out->W = W;
-        out->L = static_cast<uint32_t>(pl.L);
-        out->K = static_cast<uint32_t>(pl.K);
-        out->logN = pl.g.logN;
-        out->logR = pl.g.logR;
-        out->logS = pl.g.logS;
-        out->device = -1;
-        out->device_bytes = fpm::device_footprint(pl);
+        const fpm::HostPlan pl = fpm::make_plan(N, W, q, static_cast<int>(L), bits);
+        fill_info(pl, W, -1, out);
         if (primes) {
             for (int j = 0; j < pl.K; ++j) primes[j] = pl.primes[j];
         }

@@ -12,15 +12,14 @@ namespace fpm {
 struct DevPoint {
     uint32_t N, logN, logR, logS;
     int L, K;
+    int lazy;                  // primes below 2^30: lazy (Harvey) butterflies
     const PrimeConsts* pc;     // K
     const uint2* dec_a;        // K x L
     const uint2* dec_b;        // K x L
     const uint2* col_f;        // K x R
     const uint2* col_i;
     const uint2* row_u_f;      // K x R x logS
-    const uint2* row_u_i;
     const uint2* row_q_f;      // K x S
-    const uint2* row_q_i;
     const uint2* full_f;       // K x N (small transforms)
     const uint2* full_i;
     const uint32_t* q;         // L

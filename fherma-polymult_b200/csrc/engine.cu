@@ -64,9 +64,8 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
         dp_.col_f = upload(pl.col_f);
         dp_.col_i = upload(pl.col_i);
         dp_.row_u_f = upload(pl.row_u_f);
-        dp_.row_u_i = upload(pl.row_u_i);
         dp_.row_q_f = upload(pl.row_q_f);
-        dp_.row_q_i = upload(pl.row_q_i);
+        dp_.lazy = pl.lazy ? 1 : 0;
         dp_.full_f = upload(pl.full_f);
         dp_.full_i = upload(pl.full_i);
         dp_.q = upload(pl.q);

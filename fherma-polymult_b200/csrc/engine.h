@@ -15,7 +15,7 @@ namespace fpm {
 class Engine {
 public:
     // Builds the plan and uploads it (throws std::runtime_error).
-    Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2 = 31);
+    Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2 = kDefaultPrimeBits);
     ~Engine();
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;

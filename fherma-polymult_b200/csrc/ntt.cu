@@ -4,10 +4,19 @@
 //
 // Reference counterparts (Akram275/fherma-polymult): k_ntt_cols solve.cu:130-166,
 // k_ntt_rows_mul solve.cu:195-233, with the stage structure of
-// rns_kernels.cuh:105-174.  Here every pass keeps 8 elements per thread in
-// registers for up to three stages at a time (ntt_engine.cuh), the row pass
-// builds its twiddles in shared memory from two small per-prime tables, and A
-// and B share each twiddle load.
+// rns_kernels.cuh:105-174.  Here (ntt_engine.cuh):
+//   * every pass keeps 8 elements per thread in registers for up to three
+//     stages at a time; the first and last rounds read and write global memory
+//     directly, shared memory carries only the exchanges between rounds;
+//   * A and B share each twiddle load, a round's 7 twiddles come in 3 vector
+//     loads;
+//   * the row pass builds only the FORWARD twiddle tables of its rows, from two
+//     small per-prime tables, and pairs row u with row R - 1 - u: the inverse
+//     twiddle of row u at entry y is minus the forward twiddle of row R - 1 - u
+//     at y with its low bits complemented (psi^(N - e) = -psi^-e), so one
+//     table set serves both directions;
+//   * with primes below 2^30 the butterflies are Harvey's lazy ones (values
+//     below 4p forward, 2p inverse).
 #include "device.cuh"
 #include "kernels.h"
 #include "ntt_engine.cuh"
@@ -16,194 +25,313 @@ namespace fpm {
 
 namespace {
 
-// ---------------------------------------------------------------------------
-// Column pass: a block owns C = 2048 / R adjacent columns c0 .. c0 + C - 1 of one
-// prime, all R rows: tile sub-transform g = column, position x = row u.
-// Element (u, c) is X[u S + c0 + c].
+template <int NSUB, int XS, class SWZ>
+using RP = Rounds<NSUB, XS, SWZ>;
 
-template <int LOGR>
-__device__ __forceinline__ void col_load(uint32_t* tile, const uint32_t* X, uint32_t S, uint32_t c0) {
-    constexpr uint32_t C = kTileCols<LOGR>;
-#pragma unroll 4
-    for (uint32_t i = threadIdx.x; i < 2048; i += kNttThreads) {
-        const uint32_t c = i & (C - 1), u = i >> (11 - LOGR);
-        tile[swz((c << LOGR) | u)] = X[static_cast<size_t>(u) * S + c0 + c];
-    }
-}
-
-template <int LOGR>
-__device__ __forceinline__ void col_store(const uint32_t* tile, uint32_t* X, uint32_t S, uint32_t c0) {
-    constexpr uint32_t C = kTileCols<LOGR>;
-#pragma unroll 4
-    for (uint32_t i = threadIdx.x; i < 2048; i += kNttThreads) {
-        const uint32_t c = i & (C - 1), u = i >> (11 - LOGR);
-        X[static_cast<size_t>(u) * S + c0 + c] = tile[swz((c << LOGR) | u)];
-    }
-}
-
-template <int NSUB, int R, int NV, class TW>
+// Round R through shared memory on NV tiles.
+template <int NSUB, int XS, class SWZ, int R, bool LAZY, int NV, class TW>
 __device__ __forceinline__ void fwd_step(uint32_t* const (&tiles)[NV], const TW& tw, uint32_t p) {
-    const uint32_t base = round_base<NSUB, R>(threadIdx.x);
+    const uint32_t base = round_base<NSUB, XS, SWZ, R>(threadIdx.x);
     uint32_t v[NV][8];
 #pragma unroll
-    for (int o = 0; o < NV; ++o) load_round<NSUB, R>(tiles[o], v[o], base);
-    fwd_round<NSUB, R, NV>(v, base, tw, p);
+    for (int o = 0; o < NV; ++o) load_round<NSUB, XS, SWZ, R>(tiles[o], v[o], base);
+    fwd_round<NSUB, XS, SWZ, R, LAZY, NV>(v, base, tw, p);
 #pragma unroll
-    for (int o = 0; o < NV; ++o) store_round<NSUB, R>(tiles[o], v[o], base);
+    for (int o = 0; o < NV; ++o) store_round<NSUB, XS, SWZ, R>(tiles[o], v[o], base);
     __syncthreads();
 }
 
-template <int NSUB, int R, class TW>
-__device__ __forceinline__ void inv_step(uint32_t* tile, const TW& tw, uint32_t p) {
-    const uint32_t base = round_base<NSUB, R>(threadIdx.x);
-    uint32_t v[8];
-    load_round<NSUB, R>(tile, v, base);
-    inv_round<NSUB, R>(v, base, tw, p);
-    store_round<NSUB, R>(tile, v, base);
-    __syncthreads();
-}
-
-// Forward rounds R .. REND - 1.
-template <int NSUB, int NV, class TW, int R, int REND>
+template <int NSUB, int XS, class SWZ, int R, int REND, bool LAZY, int NV, class TW>
 __device__ __forceinline__ void fwd_range(uint32_t* const (&tiles)[NV], const TW& tw, uint32_t p) {
     if constexpr (R < REND) {
-        fwd_step<NSUB, R, NV>(tiles, tw, p);
-        fwd_range<NSUB, NV, TW, R + 1, REND>(tiles, tw, p);
+        fwd_step<NSUB, XS, SWZ, R, LAZY, NV>(tiles, tw, p);
+        fwd_range<NSUB, XS, SWZ, R + 1, REND, LAZY, NV>(tiles, tw, p);
     }
 }
 
-// Inverse rounds R, R - 1, ..., 0.
-template <int NSUB, class TW, int R>
-__device__ __forceinline__ void inv_from(uint32_t* tile, const TW& tw, uint32_t p) {
-    if constexpr (R >= 0) {
-        inv_step<NSUB, R>(tile, tw, p);
-        inv_from<NSUB, TW, R - 1>(tile, tw, p);
+// Inverse rounds R, R - 1, ..., RLO through shared memory.
+template <int NSUB, int XS, class SWZ, int R, int RLO, bool LAZY, bool NEG, class TW>
+__device__ __forceinline__ void inv_range(uint32_t* tile, const TW& tw, uint32_t p) {
+    if constexpr (R >= RLO) {
+        const uint32_t base = round_base<NSUB, XS, SWZ, R>(threadIdx.x);
+        uint32_t v[8];
+        load_round<NSUB, XS, SWZ, R>(tile, v, base);
+        inv_round<NSUB, XS, SWZ, R, LAZY, NEG>(v, base, tw, p);
+        store_round<NSUB, XS, SWZ, R>(tile, v, base);
+        __syncthreads();
+        inv_range<NSUB, XS, SWZ, R - 1, RLO, LAZY, NEG>(tile, tw, p);
     }
 }
+
+// Canonical residue from a lazy one (< 4p).
+__device__ __forceinline__ uint32_t canon4(uint32_t x, uint32_t p) {
+    x = umin32(x, x - 2 * p);
+    return umin32(x, x - p);
+}
+
+// ---------------------------------------------------------------------------
+// Column pass: a block owns C = 2^XS adjacent columns c0 .. c0 + C - 1 of one
+// prime and all R = 2^LOGR rows; tile index i = u C + c (row u = position in the
+// sub-transform, column c = sub-transform).  Element (u, c) is X[u S + c0 + c].
 
 template <int LOGR>
+__device__ __forceinline__ size_t col_offset(uint32_t i, uint32_t S, uint32_t c0) {
+    constexpr int XS = 11 - LOGR;
+    return static_cast<size_t>(i >> XS) * S + c0 + (i & ((1u << XS) - 1u));
+}
+
+template <int LOGR, int R, int NV>
+__device__ __forceinline__ void col_global_load(const uint32_t* const (&X)[NV], uint32_t (&v)[NV][8], uint32_t base,
+                                                uint32_t S, uint32_t c0) {
+    constexpr int XS = 11 - LOGR, sh = RP<LOGR, XS, SwzCol>::lo(R);
+    const size_t at = col_offset<LOGR>(base, S, c0);
+    const size_t step = static_cast<size_t>(S) << sh;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int o = 0; o < NV; ++o) v[o][k] = X[o][at + k * step];
+}
+
+template <int LOGR, int R, int NV>
+__device__ __forceinline__ void col_global_store(uint32_t* const (&X)[NV], const uint32_t (&v)[NV][8], uint32_t base,
+                                                 uint32_t S, uint32_t c0) {
+    constexpr int XS = 11 - LOGR, sh = RP<LOGR, XS, SwzCol>::lo(R);
+    const size_t at = col_offset<LOGR>(base, S, c0);
+    const size_t step = static_cast<size_t>(S) << sh;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int o = 0; o < NV; ++o) X[o][at + k * step] = v[o][k];
+}
+
+template <int LOGR, bool LAZY>
 __global__ void __launch_bounds__(kNttThreads) k_ntt_col_fwd(DevPoint d, uint32_t* A, uint32_t* B) {
-    extern __shared__ __align__(16) uint32_t smem[];
-    constexpr uint32_t R = 1u << LOGR, C = kTileCols<LOGR>;
+    extern __shared__ __align__(1024) uint32_t smem[];
+    constexpr int XS = 11 - LOGR;
+    constexpr uint32_t R = 1u << LOGR, C = 1u << XS;
+    constexpr int last = RP<LOGR, XS, SwzCol>::kCount - 1;
     uint32_t* ta = smem;
     uint32_t* tb = smem + 2048;
     uint2* tw = reinterpret_cast<uint2*>(smem + 4096);
     const int j = blockIdx.y;
     const uint32_t S = 1u << d.logS, c0 = blockIdx.x * C;
     const uint32_t p = d.pc[j].p;
+    uint32_t* const X[2] = {A + static_cast<size_t>(j) * d.N, B + static_cast<size_t>(j) * d.N};
     for (uint32_t y = threadIdx.x; y < R; y += kNttThreads) tw[y] = d.col_f[static_cast<size_t>(j) * R + y];
-    col_load<LOGR>(ta, A + static_cast<size_t>(j) * d.N, S, c0);
-    col_load<LOGR>(tb, B + static_cast<size_t>(j) * d.N, S, c0);
-    __syncthreads();
+    const SharedTable table{tw};
     uint32_t* const tiles[2] = {ta, tb};
-    fwd_range<LOGR, 2, SharedTable, 0, Rounds<LOGR>::kCount>(tiles, SharedTable{tw}, p);
-    col_store<LOGR>(ta, A + static_cast<size_t>(j) * d.N, S, c0);
-    col_store<LOGR>(tb, B + static_cast<size_t>(j) * d.N, S, c0);
+    {
+        const uint32_t base = round_base<LOGR, XS, SwzCol, 0>(threadIdx.x);
+        uint32_t v[2][8];
+        const uint32_t* const Xc[2] = {X[0], X[1]};
+        col_global_load<LOGR, 0, 2>(Xc, v, base, S, c0);
+        __syncthreads();   // the twiddle table
+        fwd_round<LOGR, XS, SwzCol, 0, LAZY, 2>(v, base, table, p);
+#pragma unroll
+        for (int o = 0; o < 2; ++o) store_round<LOGR, XS, SwzCol, 0>(tiles[o], v[o], base);
+        __syncthreads();
+    }
+    fwd_range<LOGR, XS, SwzCol, 1, last, LAZY, 2>(tiles, table, p);
+    {
+        const uint32_t base = round_base<LOGR, XS, SwzCol, last>(threadIdx.x);
+        uint32_t v[2][8];
+#pragma unroll
+        for (int o = 0; o < 2; ++o) load_round<LOGR, XS, SwzCol, last>(tiles[o], v[o], base);
+        fwd_round<LOGR, XS, SwzCol, last, LAZY, 2>(v, base, table, p);
+        col_global_store<LOGR, last, 2>(X, v, base, S, c0);
+    }
 }
 
-template <int LOGR>
+template <int LOGR, bool LAZY>
 __global__ void __launch_bounds__(kNttThreads) k_ntt_col_inv(DevPoint d, uint32_t* A) {
-    extern __shared__ __align__(16) uint32_t smem[];
-    constexpr uint32_t R = 1u << LOGR, C = kTileCols<LOGR>;
+    extern __shared__ __align__(1024) uint32_t smem[];
+    constexpr int XS = 11 - LOGR;
+    constexpr uint32_t R = 1u << LOGR, C = 1u << XS;
+    constexpr int last = RP<LOGR, XS, SwzCol>::kCount - 1;
     uint32_t* ta = smem;
     uint2* tw = reinterpret_cast<uint2*>(smem + 2048);
     const int j = blockIdx.y;
     const uint32_t S = 1u << d.logS, c0 = blockIdx.x * C;
     const uint32_t p = d.pc[j].p;
+    uint32_t* const X[1] = {A + static_cast<size_t>(j) * d.N};
     for (uint32_t y = threadIdx.x; y < R; y += kNttThreads) tw[y] = d.col_i[static_cast<size_t>(j) * R + y];
-    col_load<LOGR>(ta, A + static_cast<size_t>(j) * d.N, S, c0);
-    __syncthreads();
-    inv_from<LOGR, SharedTable, Rounds<LOGR>::kCount - 1>(ta, SharedTable{tw}, p);
-    col_store<LOGR>(ta, A + static_cast<size_t>(j) * d.N, S, c0);
+    const SharedTable table{tw};
+    {
+        const uint32_t base = round_base<LOGR, XS, SwzCol, last>(threadIdx.x);
+        uint32_t v[1][8];
+        const uint32_t* const Xc[1] = {X[0]};
+        col_global_load<LOGR, last, 1>(Xc, v, base, S, c0);
+        __syncthreads();
+        inv_round<LOGR, XS, SwzCol, last, LAZY, false>(v[0], base, table, p);
+        store_round<LOGR, XS, SwzCol, last>(ta, v[0], base);
+        __syncthreads();
+    }
+    inv_range<LOGR, XS, SwzCol, last - 1, 1, LAZY, false>(ta, table, p);
+    {
+        const uint32_t base = round_base<LOGR, XS, SwzCol, 0>(threadIdx.x);
+        uint32_t v[1][8];
+        load_round<LOGR, XS, SwzCol, 0>(ta, v[0], base);
+        inv_round<LOGR, XS, SwzCol, 0, LAZY, false>(v[0], base, table, p);
+        if constexpr (LAZY) {
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[0][k] = reduce_once(v[0][k], p);   // y_j canonical for the CRT
+        }
+        col_global_store<LOGR, 0, 1>(X, v, base, S, c0);
+    }
 }
 
 // ---------------------------------------------------------------------------
-// Row pass: a block owns G = 2048 / S consecutive rows u0 .. u0 + G - 1 of one
-// prime (2048 contiguous elements).  It first builds each row's forward and
-// inverse twiddle tables in shared memory: entry y of row u for the stage of
-// distance 2^b is U[u][b] * Q[y] (plan.h), with its Shoup companion derived
-// from mu.
+// Row pass.  A block owns G = 2048 / S rows of one prime: tile row g < G/2 is
+// row u0 + g, tile row g >= G/2 is row R - 1 - u0 - (g - G/2), so rows g and
+// g ^ G/2 are partners (u, R - 1 - u).  With G = 1 (S = 2048) the block owns one
+// row and builds its partner's table beside its own.
+//
+// Forward table of row u, entry y in [2^lev, 2^(lev+1)), stage b = LOGS-1-lev:
+// psi^(2^b (1 + 2 bitrev(u)) + 2^(b+1+logR) bitrev(y - 2^lev)) = U[u][b] Q[y].
 
 template <int LOGS>
-__device__ __forceinline__ void row_twiddles(uint2* tf, uint2* ti, const DevPoint& d, int j, uint32_t u0) {
-    constexpr uint32_t S = 1u << LOGS;
-    const PrimeConsts pc = d.pc[j];
-    const uint32_t R = 1u << d.logR;
-    const uint2* uf = d.row_u_f + (static_cast<size_t>(j) * R + u0) * LOGS;
-    const uint2* ui = d.row_u_i + (static_cast<size_t>(j) * R + u0) * LOGS;
-    const uint2* qf = d.row_q_f + static_cast<size_t>(j) * S;
-    const uint2* qi = d.row_q_i + static_cast<size_t>(j) * S;
-    for (uint32_t i = threadIdx.x; i < 2048; i += kNttThreads) {
-        const uint32_t g = i >> LOGS, y = i & (S - 1);
-        if (y == 0) continue;
-        const uint32_t b = LOGS - 1 - (31 - __clz(y));
-        const uint2 f = uf[g * LOGS + b], fi = ui[g * LOGS + b];
-        const uint2 q1 = qf[y], q2 = qi[y];
-        tf[i] = make_twiddle(shoup(f.x, q1.x, q1.y, pc.p), pc);
-        ti[i] = make_twiddle(shoup(fi.x, q2.x, q2.y, pc.p), pc);
+struct RowGeom {
+    static constexpr uint32_t S = 1u << LOGS;
+    static constexpr uint32_t G = 2048u >> LOGS;
+    static constexpr uint32_t kSlots = G >= 2 ? G : 2;
+    static constexpr uint32_t kStride = S + 4;                 // entries; pads rows across banks
+    static constexpr uint32_t kFlip = G >= 2 ? G / 2 : 1;
+    static constexpr uint32_t kPairsPerBlock = G >= 2 ? G / 2 : 1;
+};
+
+template <int LOGS>
+__device__ __forceinline__ uint32_t row_of_slot(uint32_t slot, uint32_t u0, uint32_t R) {
+    using RG = RowGeom<LOGS>;
+    if constexpr (RG::G >= 2) {
+        return slot < RG::G / 2 ? u0 + slot : R - 1 - u0 - (slot - RG::G / 2);
+    } else {
+        return slot == 0 ? u0 : R - 1 - u0;
     }
 }
 
 template <int LOGS>
+__device__ __forceinline__ void row_tables(uint2* tf, const DevPoint& d, int j, uint32_t u0) {
+    using RG = RowGeom<LOGS>;
+    const PrimeConsts pc = d.pc[j];
+    const uint32_t R = 1u << d.logR;
+    const uint2* qf = d.row_q_f + static_cast<size_t>(j) * RG::S;
+    for (uint32_t i = threadIdx.x; i < RG::kSlots * RG::S; i += kNttThreads) {
+        const uint32_t slot = i >> LOGS, y = i & (RG::S - 1);
+        if (y == 0) continue;
+        const uint32_t u = row_of_slot<LOGS>(slot, u0, R);
+        const uint32_t b = LOGS - 1 - (31 - __clz(y));
+        const uint2 f = d.row_u_f[(static_cast<size_t>(j) * R + u) * LOGS + b];
+        const uint2 q1 = qf[y];
+        tf[slot * RG::kStride + y] = make_twiddle(shoup(f.x, q1.x, q1.y, pc.p), pc);
+    }
+}
+
+template <int LOGS>
+__device__ __forceinline__ size_t row_offset(uint32_t i, uint32_t u0, uint32_t R) {
+    return static_cast<size_t>(row_of_slot<LOGS>(i >> LOGS, u0, R)) * (1u << LOGS) + (i & ((1u << LOGS) - 1u));
+}
+
+template <int LOGS, bool LAZY>
 __global__ void __launch_bounds__(kNttThreads) k_ntt_row(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
-    extern __shared__ __align__(16) uint32_t smem[];
-    constexpr uint32_t S = 1u << LOGS, G = 2048u >> LOGS;
+    extern __shared__ __align__(1024) uint32_t smem[];
+    using RG = RowGeom<LOGS>;
+    using RPR = RP<LOGS, 0, SwzRow>;
+    constexpr int last = RPR::kCount - 1;
     uint32_t* ta = smem;
     uint32_t* tb = smem + 2048;
     uint2* tf = reinterpret_cast<uint2*>(smem + 4096);
-    uint2* ti = tf + 2048;
     const int j = blockIdx.y;
-    const uint32_t u0 = blockIdx.x * G;
+    const uint32_t u0 = blockIdx.x * RG::kPairsPerBlock;
+    const uint32_t R = 1u << d.logR;
     const PrimeConsts pc = d.pc[j];
-    uint32_t* a = A + static_cast<size_t>(j) * d.N + static_cast<size_t>(u0) * S;
-    uint32_t* b = B + static_cast<size_t>(j) * d.N + static_cast<size_t>(u0) * S;
-    row_twiddles<LOGS>(tf, ti, d, j, u0);
-#pragma unroll 4
-    for (uint32_t i = threadIdx.x; i < 2048; i += kNttThreads) {
-        ta[swz(i)] = a[i];
-        tb[swz(i)] = b[i];
-    }
-    __syncthreads();
-    using RP = Rounds<LOGS>;
-    constexpr int last = RP::kCount - 1;
-    const PerRowTable<LOGS> fw{tf}, iw{ti};
+    const uint32_t p = pc.p;
+    uint32_t* a = A + static_cast<size_t>(j) * d.N;
+    uint32_t* b = B + static_cast<size_t>(j) * d.N;
+    const RowTable<LOGS, RG::kStride, false, RG::kFlip> fw{tf};
+    const RowTable<LOGS, RG::kStride, true, RG::kFlip> iw{tf};
     uint32_t* const tiles[2] = {ta, tb};
-    // Forward rounds but the last through shared memory.
-    fwd_range<LOGS, 2, PerRowTable<LOGS>, 0, last>(tiles, fw, pc.p);
-    // The last forward round stays in registers when the product follows.
+
+    // Round 0 straight from global memory (the thread's 8 elements lie in one row).
     {
-        const uint32_t base = round_base<LOGS, last>(threadIdx.x);
+        const uint32_t base = round_base<LOGS, 0, SwzRow, 0>(threadIdx.x);
+        constexpr int sh = RPR::lo(0);
+        const size_t at = row_offset<LOGS>(base, u0, R);
         uint32_t v[2][8];
-        load_round<LOGS, last>(ta, v[0], base);
-        load_round<LOGS, last>(tb, v[1], base);
-        fwd_round<LOGS, last, 2>(v, base, fw, pc.p);
-        if (mode == kRowForward) {
-            store_round<LOGS, last>(ta, v[0], base);
-            store_round<LOGS, last>(tb, v[1], base);
-        } else {
 #pragma unroll
-            for (int k = 0; k < 8; ++k) v[0][k] = mont_mul(v[0][k], v[1][k], pc.p, pc.pneg);
-            inv_round<LOGS, last>(v[0], base, iw, pc.p);
-            store_round<LOGS, last>(ta, v[0], base);
+        for (int k = 0; k < 8; ++k) {
+            v[0][k] = a[at + (k << sh)];
+            v[1][k] = b[at + (k << sh)];
         }
+        row_tables<LOGS>(tf, d, j, u0);
+        __syncthreads();
+        fwd_round<LOGS, 0, SwzRow, 0, LAZY, 2>(v, base, fw, p);
+#pragma unroll
+        for (int o = 0; o < 2; ++o) store_round<LOGS, 0, SwzRow, 0>(tiles[o], v[o], base);
         __syncthreads();
     }
-    if (mode == kRowForward) {
-#pragma unroll 4
-        for (uint32_t i = threadIdx.x; i < 2048; i += kNttThreads) {
-            a[i] = ta[swz(i)];
-            b[i] = tb[swz(i)];
+    fwd_range<LOGS, 0, SwzRow, 1, last, LAZY, 2>(tiles, fw, p);
+    // Last forward round, the pointwise product and the first inverse round in
+    // registers.
+    {
+        const uint32_t base = round_base<LOGS, 0, SwzRow, last>(threadIdx.x);
+        uint32_t v[2][8];
+        load_round<LOGS, 0, SwzRow, last>(ta, v[0], base);
+        load_round<LOGS, 0, SwzRow, last>(tb, v[1], base);
+        fwd_round<LOGS, 0, SwzRow, last, LAZY, 2>(v, base, fw, p);
+        if (mode == kRowForward) {
+            if constexpr (LAZY) {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    v[0][k] = canon4(v[0][k], p);
+                    v[1][k] = canon4(v[1][k], p);
+                }
+            }
+            store_round<LOGS, 0, SwzRow, last>(ta, v[0], base);
+            store_round<LOGS, 0, SwzRow, last>(tb, v[1], base);
+            __syncthreads();
+            for (uint32_t i = threadIdx.x; i < 2048; i += kNttThreads) {
+                const size_t at = row_offset<LOGS>(i, u0, R);
+                a[at] = ta[SwzRow::f(i)];
+                b[at] = tb[SwzRow::f(i)];
+            }
+            return;
         }
-        return;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            uint32_t x = v[0][k], y = v[1][k];
+            if constexpr (LAZY) {
+                // below 2p each, so the Montgomery product stays below 2p
+                x = umin32(x, x - 2 * p);
+                y = umin32(y, y - 2 * p);
+            }
+            v[0][k] = mont_mul(x, y, p, pc.pneg);
+        }
+        inv_round<LOGS, 0, SwzRow, last, LAZY, true>(v[0], base, iw, p);
+        store_round<LOGS, 0, SwzRow, last>(ta, v[0], base);
+        __syncthreads();
     }
-    if constexpr (last > 0) inv_from<LOGS, PerRowTable<LOGS>, last - 1>(ta, iw, pc.p);
-#pragma unroll 4
-    for (uint32_t i = threadIdx.x; i < 2048; i += kNttThreads) a[i] = ta[swz(i)];
+    inv_range<LOGS, 0, SwzRow, last - 1, 1, LAZY, true>(ta, iw, p);
+    // Inverse round 0 straight to global memory.
+    {
+        const uint32_t base = round_base<LOGS, 0, SwzRow, 0>(threadIdx.x);
+        constexpr int sh = RPR::lo(0);
+        uint32_t v[8];
+        load_round<LOGS, 0, SwzRow, 0>(ta, v, base);
+        inv_round<LOGS, 0, SwzRow, 0, LAZY, true>(v, base, iw, p);
+        if (LAZY && d.logR == 0) {
+            // No column pass follows: these are the y_j, canonical for the CRT.
+#pragma unroll
+            for (int k = 0; k < 8; ++k) v[k] = reduce_once(v[k], p);
+        }
+        const size_t at = row_offset<LOGS>(base, u0, R);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[at + (k << sh)] = v[k];
+    }
 }
 
 // ---------------------------------------------------------------------------
 // N <= 1024: one block per prime holds both operands; one butterfly per
-// thread per stage, full twiddle tables from global memory.
+// thread per stage, full twiddle tables from global memory, full reduction.
 
 __global__ void __launch_bounds__(kNttThreads) k_ntt_small(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
     extern __shared__ __align__(16) uint32_t smem[];
@@ -249,100 +377,122 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_small(DevPoint d, uint32_t*
     for (uint32_t i = threadIdx.x; i < N; i += blockDim.x) a[i] = ta[i];
 }
 
-template <int LOGR>
-void set_col_attrs() {
-    check(cudaFuncSetAttribute(k_ntt_col_fwd<LOGR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(col_fwd_smem(LOGR))),
+size_t col_fwd_smem_t(uint32_t logR) { return 2 * 2048 * sizeof(uint32_t) + (size_t(1) << logR) * sizeof(uint2); }
+size_t col_inv_smem_t(uint32_t logR) { return 2048 * sizeof(uint32_t) + (size_t(1) << logR) * sizeof(uint2); }
+
+template <int LOGS>
+constexpr size_t row_smem_t() {
+    return 2 * 2048 * sizeof(uint32_t) + RowGeom<LOGS>::kSlots * RowGeom<LOGS>::kStride * sizeof(uint2);
+}
+
+template <int LOGR, bool LAZY>
+void col_attrs() {
+    check(cudaFuncSetAttribute(k_ntt_col_fwd<LOGR, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(col_fwd_smem_t(LOGR))),
           "col smem");
-    check(cudaFuncSetAttribute(k_ntt_col_inv<LOGR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(col_inv_smem(LOGR))),
+    check(cudaFuncSetAttribute(k_ntt_col_inv<LOGR, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(col_inv_smem_t(LOGR))),
           "col smem");
 }
 
-template <int LOGS>
-void set_row_attrs() {
-    check(cudaFuncSetAttribute(k_ntt_row<LOGS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(row_smem())),
+template <int LOGS, bool LAZY>
+void row_attrs() {
+    check(cudaFuncSetAttribute(k_ntt_row<LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(row_smem_t<LOGS>())),
           "row smem");
 }
 
-template <int LOGR>
+template <bool LAZY>
+void attrs_all() {
+    col_attrs<6, LAZY>();
+    col_attrs<7, LAZY>();
+    col_attrs<8, LAZY>();
+    col_attrs<9, LAZY>();
+    col_attrs<10, LAZY>();
+    col_attrs<11, LAZY>();
+    row_attrs<6, LAZY>();
+    row_attrs<7, LAZY>();
+    row_attrs<8, LAZY>();
+    row_attrs<9, LAZY>();
+    row_attrs<10, LAZY>();
+    row_attrs<11, LAZY>();
+}
+
+template <int LOGR, bool LAZY>
 void launch_col_fwd_t(const DevPoint& d, uint32_t* A, uint32_t* B, cudaStream_t st) {
-    const dim3 grid((1u << d.logS) / kTileCols<LOGR>, d.K);
-    k_ntt_col_fwd<LOGR><<<grid, kNttThreads, col_fwd_smem(LOGR), st>>>(d, A, B);
+    const dim3 grid((1u << d.logS) >> (11 - LOGR), d.K);
+    k_ntt_col_fwd<LOGR, LAZY><<<grid, kNttThreads, col_fwd_smem_t(LOGR), st>>>(d, A, B);
 }
 
-template <int LOGR>
+template <int LOGR, bool LAZY>
 void launch_col_inv_t(const DevPoint& d, uint32_t* A, cudaStream_t st) {
-    const dim3 grid((1u << d.logS) / kTileCols<LOGR>, d.K);
-    k_ntt_col_inv<LOGR><<<grid, kNttThreads, col_inv_smem(LOGR), st>>>(d, A);
+    const dim3 grid((1u << d.logS) >> (11 - LOGR), d.K);
+    k_ntt_col_inv<LOGR, LAZY><<<grid, kNttThreads, col_inv_smem_t(LOGR), st>>>(d, A);
 }
 
-template <int LOGS>
+template <int LOGS, bool LAZY>
 void launch_row_t(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStream_t st) {
-    const dim3 grid((1u << d.logR) / (2048u >> LOGS), d.K);
-    k_ntt_row<LOGS><<<grid, kNttThreads, row_smem(), st>>>(d, A, B, mode);
+    using RG = RowGeom<LOGS>;
+    const uint32_t R = 1u << d.logR;
+    const dim3 grid(RG::G >= 2 ? R / RG::G : R, d.K);
+    k_ntt_row<LOGS, LAZY><<<grid, kNttThreads, row_smem_t<LOGS>(), st>>>(d, A, B, mode);
 }
 
-}  // namespace
-
-size_t col_fwd_smem(uint32_t logR) { return 2 * 2048 * sizeof(uint32_t) + (size_t(1) << logR) * sizeof(uint2); }
-size_t col_inv_smem(uint32_t logR) { return 2048 * sizeof(uint32_t) + (size_t(1) << logR) * sizeof(uint2); }
-size_t row_smem() { return 2 * 2048 * sizeof(uint32_t) + 2 * 2048 * sizeof(uint2); }
-
-void ntt_init_attributes() {
-    set_col_attrs<6>();
-    set_col_attrs<7>();
-    set_col_attrs<8>();
-    set_col_attrs<9>();
-    set_col_attrs<10>();
-    set_col_attrs<11>();
-    set_row_attrs<6>();
-    set_row_attrs<7>();
-    set_row_attrs<8>();
-    set_row_attrs<9>();
-    set_row_attrs<10>();
-    set_row_attrs<11>();
-    check(cudaFuncSetAttribute(k_ntt_small, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 1024 * 4),
-          "small smem");
-}
-
-// The product's transform chain on residues A, B (K x N each): y_j in A.
-// mode kRowForward stops after the forward transforms (A, B bit-reversed).
-void launch_ntt(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStream_t st) {
-    if (d.logN <= kSmallLogN) {
-        k_ntt_small<<<d.K, kNttThreads, 2 * d.N * sizeof(uint32_t), st>>>(d, A, B, mode);
-        return;
-    }
+template <bool LAZY>
+void launch_ntt_t(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStream_t st) {
     switch (d.logR) {
         case 0: break;
-        case 6: launch_col_fwd_t<6>(d, A, B, st); break;
-        case 7: launch_col_fwd_t<7>(d, A, B, st); break;
-        case 8: launch_col_fwd_t<8>(d, A, B, st); break;
-        case 9: launch_col_fwd_t<9>(d, A, B, st); break;
-        case 10: launch_col_fwd_t<10>(d, A, B, st); break;
-        case 11: launch_col_fwd_t<11>(d, A, B, st); break;
+        case 6: launch_col_fwd_t<6, LAZY>(d, A, B, st); break;
+        case 7: launch_col_fwd_t<7, LAZY>(d, A, B, st); break;
+        case 8: launch_col_fwd_t<8, LAZY>(d, A, B, st); break;
+        case 9: launch_col_fwd_t<9, LAZY>(d, A, B, st); break;
+        case 10: launch_col_fwd_t<10, LAZY>(d, A, B, st); break;
+        case 11: launch_col_fwd_t<11, LAZY>(d, A, B, st); break;
         default: throw std::runtime_error("unsupported column length");
     }
     switch (d.logS) {
-        case 6: launch_row_t<6>(d, A, B, mode, st); break;
-        case 7: launch_row_t<7>(d, A, B, mode, st); break;
-        case 8: launch_row_t<8>(d, A, B, mode, st); break;
-        case 9: launch_row_t<9>(d, A, B, mode, st); break;
-        case 10: launch_row_t<10>(d, A, B, mode, st); break;
-        case 11: launch_row_t<11>(d, A, B, mode, st); break;
+        case 6: launch_row_t<6, LAZY>(d, A, B, mode, st); break;
+        case 7: launch_row_t<7, LAZY>(d, A, B, mode, st); break;
+        case 8: launch_row_t<8, LAZY>(d, A, B, mode, st); break;
+        case 9: launch_row_t<9, LAZY>(d, A, B, mode, st); break;
+        case 10: launch_row_t<10, LAZY>(d, A, B, mode, st); break;
+        case 11: launch_row_t<11, LAZY>(d, A, B, mode, st); break;
         default: throw std::runtime_error("unsupported row length");
     }
     if (mode == kRowForward) return;
     switch (d.logR) {
         case 0: break;
-        case 6: launch_col_inv_t<6>(d, A, st); break;
-        case 7: launch_col_inv_t<7>(d, A, st); break;
-        case 8: launch_col_inv_t<8>(d, A, st); break;
-        case 9: launch_col_inv_t<9>(d, A, st); break;
-        case 10: launch_col_inv_t<10>(d, A, st); break;
-        case 11: launch_col_inv_t<11>(d, A, st); break;
+        case 6: launch_col_inv_t<6, LAZY>(d, A, st); break;
+        case 7: launch_col_inv_t<7, LAZY>(d, A, st); break;
+        case 8: launch_col_inv_t<8, LAZY>(d, A, st); break;
+        case 9: launch_col_inv_t<9, LAZY>(d, A, st); break;
+        case 10: launch_col_inv_t<10, LAZY>(d, A, st); break;
+        case 11: launch_col_inv_t<11, LAZY>(d, A, st); break;
         default: throw std::runtime_error("unsupported column length");
+    }
+}
+
+}  // namespace
+
+void ntt_init_attributes() {
+    attrs_all<true>();
+    attrs_all<false>();
+    check(cudaFuncSetAttribute(k_ntt_small, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 1024 * 4),
+          "small smem");
+}
+
+// The product's transform chain on residues A, B (K x N each): y_j in A.
+// mode kRowForward stops after the forward transforms (A, B bit-reversed,
+// canonical).
+void launch_ntt(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStream_t st) {
+    if (d.logN <= kSmallLogN) {
+        k_ntt_small<<<d.K, kNttThreads, 2 * d.N * sizeof(uint32_t), st>>>(d, A, B, mode);
+        return;
+    }
+    if (d.lazy) {
+        launch_ntt_t<true>(d, A, B, mode, st);
+    } else {
+        launch_ntt_t<false>(d, A, B, mode, st);
     }
 }
 

@@ -94,7 +94,7 @@ Geometry make_geometry(uint32_t logN) {
 size_t device_footprint(const HostPlan& pl) {
     auto bytes = [](const auto& v) { return v.size() * sizeof(v[0]); };
     size_t t = bytes(pl.pc) + bytes(pl.dec_a) + bytes(pl.dec_b) + bytes(pl.col_f) + bytes(pl.col_i) +
-               bytes(pl.row_u_f) + bytes(pl.row_u_i) + bytes(pl.row_q_f) + bytes(pl.row_q_i) +
+               bytes(pl.row_u_f) + bytes(pl.row_q_f) +
                bytes(pl.full_f) + bytes(pl.full_i) + bytes(pl.q) + bytes(pl.M) + bytes(pl.negvP) +
                bytes(pl.p_recip) + bytes(pl.dec_img_a) + bytes(pl.dec_img_b) + bytes(pl.dec_fold) +
                bytes(pl.crt_img) + sizeof(uint32_t);
@@ -117,6 +117,7 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
     pl.W = W;
     pl.L = L;
     pl.pmax_log2 = pmax_log2;
+    pl.lazy = pmax_log2 <= 30;
     uint32_t logN = 0;
     while ((1u << logN) < N) ++logN;
     pl.g = make_geometry(logN);
@@ -161,9 +162,7 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
         pl.full_i.resize(static_cast<size_t>(K) * N);
     } else {
         pl.row_u_f.resize(static_cast<size_t>(K) * R * g.logS);
-        pl.row_u_i.resize(static_cast<size_t>(K) * R * g.logS);
         pl.row_q_f.resize(static_cast<size_t>(K) * S);
-        pl.row_q_i.resize(static_cast<size_t>(K) * S);
         if (g.logR) {
             pl.col_f.resize(static_cast<size_t>(K) * R);
             pl.col_i.resize(static_cast<size_t>(K) * R);
@@ -224,7 +223,6 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
                 const uint64_t e = (1ull << b) * (1 + 2ull * bitrev(u, g.logR));
                 const size_t at = (static_cast<size_t>(j) * R + u) * g.logS + b;
                 pl.row_u_f[at] = pair(pow_mod(psi, e, p), p);
-                pl.row_u_i[at] = pair(pow_mod(ipsi, e, p), p);
             }
         }
         for (uint32_t y = 1; y < S; ++y) {
@@ -234,7 +232,6 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
             const uint32_t r = y - (1u << lev);
             const uint64_t e = (1ull << (b + 1 + g.logR)) * bitrev(r, lev);
             pl.row_q_f[static_cast<size_t>(j) * S + y] = pair(pow_mod(psi, e, p), p);
-            pl.row_q_i[static_cast<size_t>(j) * S + y] = pair(pow_mod(ipsi, e, p), p);
         }
     }
 

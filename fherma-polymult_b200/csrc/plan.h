@@ -40,7 +40,8 @@ struct HostPlan {
     Geometry g;
     std::vector<uint32_t> q;      // L
     double q_top = 0;             // top limbs of q as a double
-    int pmax_log2 = 31;
+    int pmax_log2 = 30;           // primes below 2^pmax_log2
+    bool lazy = true;             // pmax_log2 <= 30: lazy butterflies
 
     std::vector<uint32_t> primes;            // K
     std::vector<PrimeConsts> pc;             // K
@@ -55,11 +56,12 @@ struct HostPlan {
     // Column pass twiddles (logN >= 12): psi^(S bitrev_logR(y)) for y in [1, R),
     // K x R pairs (entry 0 unused); inverse with psi^-1.
     std::vector<uint2> col_f, col_i;
-    // Row pass twiddle generators: the twiddle of stage b (distance 2^b) for
-    // row u and group r' is psi^(2^b (1 + 2 bitrev_logR(u)) + 2^(b+1+logR) bitrev(r')),
-    // = U[u][b] * Q[y] with y = 2^(logS-1-b) + r'.
-    //   row_u_*: K x R x logS pairs, row_q_*: K x S pairs (entry 0 unused).
-    std::vector<uint2> row_u_f, row_u_i, row_q_f, row_q_i;
+    // Row pass twiddle generators: the forward twiddle of stage b (distance 2^b)
+    // for row u and group r' is psi^(2^b (1 + 2 bitrev_logR(u)) + 2^(b+1+logR) bitrev(r'))
+    // = U[u][b] * Q[y] with y = 2^(logS-1-b) + r'.  (The inverse twiddles are
+    // negated forward ones of the partner row R - 1 - u, see ntt.cu.)
+    //   row_u_f: K x R x logS pairs, row_q_f: K x S pairs (entry 0 unused).
+    std::vector<uint2> row_u_f, row_q_f;
     // Small transforms (logN <= kSmallLogN): psi^bitrev_logN(y), K x N pairs.
     std::vector<uint2> full_f, full_i;
 
@@ -96,6 +98,10 @@ size_t device_footprint(const HostPlan& pl);
 
 // Throws std::runtime_error on an out-of-range point (N not a power of two in
 // [2, 2^22], L outside [1, 64], q's top limb zero, not enough primes).
-HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2 = 31);
+// pmax_log2 = 30 (default) keeps every prime below 2^30, which the lazy
+// butterflies need; 31 reproduces the reference's prime set exactly
+// (rns_plan.h:141-153) and uses fully reduced butterflies.
+constexpr int kDefaultPrimeBits = 30;
+HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2 = kDefaultPrimeBits);
 
 }  // namespace fpm

@@ -38,7 +38,7 @@ _u32p = ctypes.POINTER(ctypes.c_uint32)
 class FpmInfo(ctypes.Structure):
     _fields_ = [("N", ctypes.c_uint32), ("W", ctypes.c_uint32), ("L", ctypes.c_uint32), ("K", ctypes.c_uint32),
                 ("logN", ctypes.c_uint32), ("logR", ctypes.c_uint32), ("logS", ctypes.c_uint32),
-                ("device", ctypes.c_int32), ("device_bytes", ctypes.c_uint64)]
+                ("device", ctypes.c_int32), ("device_bytes", ctypes.c_uint64), ("prime_bits", ctypes.c_uint32)]
 
 
 class FpmError(RuntimeError):
@@ -62,6 +62,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     vp = ctypes.c_void_p
     sig = {
         "fpm_init": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u32p, ctypes.POINTER(vp)], ctypes.c_int),
+        "fpm_init_ex": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u32p, ctypes.c_int, ctypes.POINTER(vp)],
+                        ctypes.c_int),
+        "fpm_plan_info_ex": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u32p, ctypes.c_int,
+                              ctypes.POINTER(FpmInfo), _u32p], ctypes.c_int),
         "fpm_run": ([vp, vp, vp, vp], ctypes.c_int),
         "fpm_run_device": ([vp, vp, vp, vp, vp], ctypes.c_int),
         "fpm_free": ([vp], None),
@@ -95,31 +99,34 @@ def _limbs(x, rows: int, L: int, name: str) -> np.ndarray:
     return x.reshape(rows, L)
 
 
-def plan_info(N: int, W: int, q) -> tuple[FpmInfo, np.ndarray]:
+def plan_info(N: int, W: int, q, prime_bits: int = 0) -> tuple[FpmInfo, np.ndarray]:
     """Host-only: the plan fherma_init would build (raises on a bad point)."""
     lib = load()
     q = np.ascontiguousarray(q, dtype=np.uint32)
     info = FpmInfo()
     primes = np.zeros(160, np.uint32)
-    _check(lib.fpm_plan_info(N, W, q.shape[0], q.ctypes.data_as(_u32p), ctypes.byref(info),
-                             primes.ctypes.data_as(_u32p)))
+    _check(lib.fpm_plan_info_ex(N, W, q.shape[0], q.ctypes.data_as(_u32p), prime_bits, ctypes.byref(info),
+                                primes.ctypes.data_as(_u32p)))
     return info, primes[:info.K].copy()
 
 
 class Context:
     """One point's resident state on the current CUDA device (fpm_ctx)."""
 
-    def __init__(self, N: int, W: int, q):
+    def __init__(self, N: int, W: int, q, prime_bits: int = 0):
+        """prime_bits: 30 (primes below 2^30, the default) or 31 (the reference's
+        prime set); 0 takes the default."""
         lib = load()
         q = np.ascontiguousarray(q, dtype=np.uint32)
         h = ctypes.c_void_p()
-        _check(lib.fpm_init(N, W, q.shape[0], q.ctypes.data_as(_u32p), ctypes.byref(h)))
+        _check(lib.fpm_init_ex(N, W, q.shape[0], q.ctypes.data_as(_u32p), prime_bits, ctypes.byref(h)))
         self._h = h
         self._lib = lib
         info = FpmInfo()
         _check(lib.fpm_get_info(h, ctypes.byref(info)))
         self.info = info
         self.N, self.W, self.L, self.K = info.N, W, info.L, info.K
+        self.prime_bits = info.prime_bits
 
     def close(self):
         if getattr(self, "_h", None):

@@ -47,6 +47,7 @@ typedef struct fpm_info {
     uint32_t logN, logR, logS; /* transform geometry: N = 2^logR x 2^logS */
     int32_t device;       /* CUDA device the context lives on (-1: host-only query) */
     uint64_t device_bytes; /* device memory the context holds: tables + workspaces */
+    uint32_t prime_bits;  /* every prime is below 2^prime_bits */
 } fpm_info;
 
 /* Replaces fherma_init (reference fherma.h:46, solve.cu:710-869): builds the
@@ -54,6 +55,13 @@ typedef struct fpm_info {
  * current CUDA device.  q has L limbs with a nonzero top limb; N is a power of
  * two in [2, 2^22]; 1 <= L <= 64.  W is recorded, as the reference does. */
 FPM_API int fpm_init(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, fpm_ctx** out);
+
+/* fpm_init with the RNS prime window chosen explicitly: prime_bits = 30 keeps
+ * every prime below 2^30 (lazy butterflies, the default), 31 reproduces the
+ * reference's prime set exactly (rns_plan.h:141-153); 0 means the default,
+ * which the environment variable FPM_PRIME_BITS may override.  Results are
+ * identical either way. */
+FPM_API int fpm_init_ex(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int prime_bits, fpm_ctx** out);
 
 /* Replaces fherma_run (reference fherma.h:47, solve.cu:871-1059): one product
  * on HOST buffers a, b, c (N x L u32 each, any host memory); returns when c is
@@ -77,6 +85,8 @@ FPM_API int fpm_get_info(const fpm_ctx* ctx, fpm_info* out);
  * out (device = -1) and, if primes is not NULL, the K primes.  Used to check a
  * point and to size its device footprint before admitting it. */
 FPM_API int fpm_plan_info(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, fpm_info* out, uint32_t* primes);
+FPM_API int fpm_plan_info_ex(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int prime_bits, fpm_info* out,
+                             uint32_t* primes);
 /* The K primes of the RNS basis, in order (same set and order as the
  * reference's make_plan, rns_plan.h:138-153). */
 FPM_API int fpm_get_primes(const fpm_ctx* ctx, uint32_t* out);

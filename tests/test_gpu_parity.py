@@ -45,8 +45,18 @@ def scaled(pl, res, N):
 
 @pytest.mark.parametrize("entry", CASES, ids=[c["file"][:-4] for c in CASES])
 def test_golden_vectors(cuda, entry):
+    """Default prime window (p < 2^30): same products as the reference."""
     g = load_golden(entry)
     with polymul.Context(entry["N"], entry["W"], g["q"]) as ctx:
+        assert ctx.prime_bits == 30
+        assert np.array_equal(ctx.run(g["a"], g["b"]), g["c"])
+
+
+@pytest.mark.parametrize("entry", CASES[::2], ids=[c["file"][:-4] for c in CASES[::2]])
+def test_golden_vectors_reference_primes(cuda, entry):
+    """prime_bits = 31: the reference's own prime set, bit for bit."""
+    g = load_golden(entry)
+    with polymul.Context(entry["N"], entry["W"], g["q"], prime_bits=31) as ctx:
         assert ctx.K == int(g["K"])
         assert np.array_equal(ctx.primes, g["primes"])
         assert np.array_equal(ctx.run(g["a"], g["b"]), g["c"])
@@ -56,12 +66,14 @@ GEOMETRIES = [(2, 33), (8, 97), (64, 100), (512, 250), (1024, 512), (2048, 129),
               (16384, 300), (32768, 868), (65536, 2048), (1 << 17, 512)]
 
 
+@pytest.mark.parametrize("prime_bits", [30, 31])
 @pytest.mark.parametrize("N,W", GEOMETRIES)
-def test_stages_match_oracle(cuda, N, W):
+def test_stages_match_oracle(cuda, N, W, prime_bits):
     torch = cuda
     q, a, b = wl.case(N, W, "uniform", seed=N + W)
-    pl = oracle.OraclePlan(N, q)
-    with polymul.Context(N, W, q) as ctx:
+    pl = oracle.OraclePlan(N, q, pmax_log2=prime_bits)
+    with polymul.Context(N, W, q, prime_bits=prime_bits) as ctx:
+        assert np.array_equal(ctx.primes, pl.primes)
         K = ctx.K
         da, db = dev(torch, a), dev(torch, b)
         A = torch.zeros((K, N), dtype=torch.int32, device="cuda")
@@ -102,6 +114,9 @@ def test_full_size_products(cuda, N, W, pattern):
     expect = oracle.OraclePlan(N, q).polymul(a, b)
     with polymul.Context(N, W, q) as ctx:
         assert np.array_equal(ctx.run(a, b), expect)
+    if pattern == "max":
+        with polymul.Context(N, W, q, prime_bits=31) as ctx:
+            assert np.array_equal(ctx.run(a, b), expect)
 
 
 def test_device_path_matches_host_path_and_repeats(cuda):

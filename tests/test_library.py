@@ -39,10 +39,14 @@ def test_library_exports_every_declared_symbol():
                                  (8192, 512), (32768, 868), (65536, 1747), (65536, 2048), (1 << 17, 512)])
 def test_plan_primes_match_oracle(N, W):
     q, _, _ = wl.case(2, W, "zero", seed=N ^ W)
+    for bits in (30, 31):
+        info, primes = polymul.plan_info(N, W, q, prime_bits=bits)
+        pl = oracle.OraclePlan(N, q, pmax_log2=bits)
+        assert info.K == pl.K and info.prime_bits == bits
+        assert np.array_equal(primes, pl.primes)
+        assert int(primes.max()) < 2**bits
     info, primes = polymul.plan_info(N, W, q)
-    pl = oracle.OraclePlan(N, q)
-    assert info.K == pl.K
-    assert np.array_equal(primes, pl.primes)
+    assert info.prime_bits == 30
     assert info.N == N and info.L == q.shape[0]
     assert info.logR + info.logS == info.logN == N.bit_length() - 1
     assert info.device == -1
