@@ -215,14 +215,23 @@ __device__ __forceinline__ void row_tables(uint2* tf, const DevPoint& d, int j, 
     const PrimeConsts pc = d.pc[j];
     const uint32_t R = 1u << d.logR;
     const uint2* qf = d.row_q_f + static_cast<size_t>(j) * RG::S;
-    for (uint32_t i = threadIdx.x; i < RG::kSlots * RG::S; i += kNttThreads) {
+    constexpr uint32_t kPer = RG::kSlots * RG::S / kNttThreads;   // 8, or 16 when G = 1
+    // Every generator load first, then the arithmetic (the loads are independent).
+    uint2 f[kPer], q1[kPer];
+#pragma unroll
+    for (uint32_t t = 0; t < kPer; ++t) {
+        const uint32_t i = threadIdx.x + t * kNttThreads;
         const uint32_t slot = i >> LOGS, y = i & (RG::S - 1);
-        if (y == 0) continue;
         const uint32_t u = row_of_slot<LOGS>(slot, u0, R);
-        const uint32_t b = LOGS - 1 - (31 - __clz(y));
-        const uint2 f = d.row_u_f[(static_cast<size_t>(j) * R + u) * LOGS + b];
-        const uint2 q1 = qf[y];
-        tf[slot * RG::kStride + y] = make_twiddle(shoup(f.x, q1.x, q1.y, pc.p), pc);
+        const uint32_t b = y ? LOGS - 1 - (31 - __clz(y)) : 0;
+        f[t] = __ldg(d.row_u_f + (static_cast<size_t>(j) * R + u) * LOGS + b);
+        q1[t] = __ldg(qf + y);
+    }
+#pragma unroll
+    for (uint32_t t = 0; t < kPer; ++t) {
+        const uint32_t i = threadIdx.x + t * kNttThreads;
+        const uint32_t slot = i >> LOGS, y = i & (RG::S - 1);
+        if (y) tf[slot * RG::kStride + y] = make_twiddle(shoup(f[t].x, q1[t].x, q1[t].y, pc.p), pc);
     }
 }
 
@@ -232,7 +241,7 @@ __device__ __forceinline__ size_t row_offset(uint32_t i, uint32_t u0, uint32_t R
 }
 
 template <int LOGS, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads) k_ntt_row(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
+__global__ void __launch_bounds__(kNttThreads, 5) k_ntt_row(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
     extern __shared__ __align__(1024) uint32_t smem[];
     using RG = RowGeom<LOGS>;
     using RPR = RP<LOGS, 0, SwzRow>;

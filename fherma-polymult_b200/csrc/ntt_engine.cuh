@@ -87,17 +87,32 @@ struct Rounds {
     }
 };
 
-// Logical index of element 0 of this thread in round R.
-template <int NSUB, int XS, class SWZ, int R>
-__device__ __forceinline__ uint32_t round_base(uint32_t tid) {
+// Bits of the lane (BITS = 5) or warp (BITS = 3) index that move by SH places.
+template <int NSUB, int XS, class SWZ, int R, bool LANE>
+__host__ __device__ constexpr uint32_t deposit_mask(int sh) {
     constexpr RoundMap m = Rounds<NSUB, XS, SWZ>::map(R);
-    const uint32_t lane = tid & 31u, warp = tid >> 5;
+    uint32_t mask = 0;
+    for (int c = 0; c < (LANE ? 5 : 3); ++c)
+        if ((LANE ? m.lane[c] : m.warp[c]) - c == sh) mask |= 1u << c;
+    return mask;
+}
+
+template <int NSUB, int XS, class SWZ, int R, bool LANE>
+__device__ __forceinline__ uint32_t deposit(uint32_t x) {
     uint32_t b = 0;
 #pragma unroll
-    for (int c = 0; c < 5; ++c) b |= ((lane >> c) & 1u) << m.lane[c];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) b |= ((warp >> c) & 1u) << m.warp[c];
+    for (int sh = 0; sh <= 10; ++sh) {
+        const uint32_t mask = deposit_mask<NSUB, XS, SWZ, R, LANE>(sh);
+        if (mask) b |= (x & mask) << sh;
+    }
     return b;
+}
+
+// Logical index of element 0 of this thread in round R (lane bits and warp
+// bits deposited group-wise: bits that move by the same distance move together).
+template <int NSUB, int XS, class SWZ, int R>
+__device__ __forceinline__ uint32_t round_base(uint32_t tid) {
+    return deposit<NSUB, XS, SWZ, R, true>(tid & 31u) | deposit<NSUB, XS, SWZ, R, false>(tid >> 5);
 }
 
 template <int NSUB, int XS, class SWZ, int R>
