@@ -13,6 +13,7 @@
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <thread>
 
 struct fpm_ctx {
     fpm::Engine* engine;
@@ -185,9 +186,28 @@ fherma::Outputs fherma_run(void* state, const fherma::Inputs& in) {
     }
     fherma::Outputs out;
     out.c.shape = {static_cast<int64_t>(pl.N), static_cast<int64_t>(pl.L)};
-    out.c.data.resize(words);
-    if (fpm_run(ctx, in.a.data.data(), in.b.data.data(), out.c.data.data()) != FPM_OK)
-        throw std::runtime_error(fpm_last_error());
+    // The answer's vector is sized (a zero fill of N L words) on a helper
+    // thread while the GPU works; run_host asks for it only when the first
+    // result chunk is ready to be copied out.
+    struct Filler {
+        std::vector<uint32_t>* v;
+        size_t n;
+        std::thread t;
+        ~Filler() {
+            if (t.joinable()) t.join();
+        }
+    } filler{&out.c.data, words, {}};
+    filler.t = std::thread([&filler] { filler.v->resize(filler.n); });
+    const int rc = guarded([&] {
+        ctx->engine->run_host(in.a.data.data(), in.b.data.data(), nullptr,
+                              [](void* p) -> uint32_t* {
+                                  auto* f = static_cast<Filler*>(p);
+                                  f->t.join();
+                                  return f->v->data();
+                              },
+                              &filler);
+    });
+    if (rc != FPM_OK) throw std::runtime_error(fpm_last_error());
     return out;
 }
 

@@ -29,15 +29,15 @@ size_t crt_smem_bytes(int L) {
 }
 
 __global__ void __launch_bounds__(kCrtThreads)
-    k_crt_simt(DevPoint d, const uint32_t* __restrict__ Y, uint32_t* __restrict__ C) {
+    k_crt_simt(DevPoint d, const uint32_t* __restrict__ Y, uint32_t* __restrict__ C, uint32_t n_begin, uint32_t n_end) {
     extern __shared__ __align__(16) uint64_t crt_smem[];
     uint64_t* part = crt_smem;                                          // [8][32][9]
     double* frac = reinterpret_cast<double*>(part + 8 * kCrtCoeffs * (kCrtChunk + 1));
     uint32_t* xw = reinterpret_cast<uint32_t*>(frac + kCrtCoeffs);      // [32][L + 2]
     const int L = d.L, K = d.K;
     const int chunks = (L + kCrtChunk - 1) / kCrtChunk;
-    const uint32_t n0 = blockIdx.x * kCrtCoeffs;
-    const uint32_t nk = min(static_cast<uint32_t>(kCrtCoeffs), d.N - n0);
+    const uint32_t n0 = n_begin + blockIdx.x * kCrtCoeffs;
+    const uint32_t nk = min(static_cast<uint32_t>(kCrtCoeffs), n_end - n0);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t n = n0 + lane;
 
@@ -100,9 +100,11 @@ void crt_init_attributes() {
           "crt smem");
 }
 
-void launch_crt(const DevPoint& d, const uint32_t* Y, uint32_t* c, cudaStream_t st) {
-    const uint32_t blocks = (d.N + kCrtCoeffs - 1) / kCrtCoeffs;
-    k_crt_simt<<<blocks, kCrtThreads, crt_smem_bytes(d.L), st>>>(d, Y, c);
+void launch_crt(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_begin, uint32_t n_end,
+                cudaStream_t st) {
+    if (n_end <= n_begin) return;
+    const uint32_t blocks = (n_end - n_begin + kCrtCoeffs - 1) / kCrtCoeffs;
+    k_crt_simt<<<blocks, kCrtThreads, crt_smem_bytes(d.L), st>>>(d, Y, c, n_begin, n_end);
 }
 
 }  // namespace fpm

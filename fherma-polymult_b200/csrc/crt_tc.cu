@@ -76,14 +76,14 @@ __device__ inline Smem carve(uint8_t* base, uint32_t u) {
 constexpr int kX = kMaxL + 2;   // register limbs of the epilogue (predicated to L + 2)
 
 __global__ void __launch_bounds__(kThreads, 1)
-    k_crt_tc(DevPoint d, const uint32_t* __restrict__ Y, uint32_t* __restrict__ C) {
+    k_crt_tc(DevPoint d, const uint32_t* __restrict__ Y, uint32_t* __restrict__ C, uint32_t n_begin, uint32_t n_end) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const uint32_t U = d.crt_u;            // GEMM columns (byte positions), multiple of 32, <= 256
     const int nch = (d.K + kChunk - 1) / kChunk;
     const Smem sm = carve(smem_raw, U);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t n0 = blockIdx.x * kRows;
-    const uint32_t nk = min(kRows, d.N - n0);
+    const uint32_t n0 = n_begin + blockIdx.x * kRows;
+    const uint32_t nk = min(kRows, n_end - n0);
     const int L = d.L, K = d.K;
     const uint32_t tcols = d.crt_tmem_cols;
 
@@ -309,9 +309,11 @@ void crt_tc_init_attributes() {
           "crt_tc smem");
 }
 
-void launch_crt_tc(const DevPoint& d, const uint32_t* Y, uint32_t* c, cudaStream_t st) {
-    const uint32_t blocks = (d.N + kRows - 1) / kRows;
-    k_crt_tc<<<blocks, kThreads, smem_bytes(d.crt_u, d.crt_tmem_cols), st>>>(d, Y, c);
+void launch_crt_tc(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_begin, uint32_t n_end,
+                   cudaStream_t st) {
+    if (n_end <= n_begin) return;
+    const uint32_t blocks = (n_end - n_begin + kRows - 1) / kRows;
+    k_crt_tc<<<blocks, kThreads, smem_bytes(d.crt_u, d.crt_tmem_cols), st>>>(d, Y, c, n_begin, n_end);
 }
 
 }  // namespace fpm

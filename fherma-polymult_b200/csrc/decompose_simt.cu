@@ -20,12 +20,13 @@ constexpr int kDecThreads = 256;
 constexpr uint32_t kDecCoeffs = 128;
 
 __global__ void __launch_bounds__(kDecThreads)
-    k_decompose_simt(DevPoint d, const uint32_t* __restrict__ limbs, uint32_t* __restrict__ res, int operand) {
+    k_decompose_simt(DevPoint d, const uint32_t* __restrict__ limbs, uint32_t* __restrict__ res, int operand,
+                     uint32_t n_begin, uint32_t n_end) {
     extern __shared__ uint32_t xs[];   // kDecCoeffs rows of L + 1 words
     const int L = d.L;
     const uint32_t stride = static_cast<uint32_t>(L) + 1;
-    const uint32_t n0 = blockIdx.x * kDecCoeffs;
-    const uint32_t nk = min(kDecCoeffs, d.N - n0);
+    const uint32_t n0 = n_begin + blockIdx.x * kDecCoeffs;
+    const uint32_t nk = min(kDecCoeffs, n_end - n0);
     const uint32_t* src = limbs + static_cast<size_t>(n0) * L;
     for (uint32_t i = threadIdx.x; i < nk * L; i += kDecThreads) {
         const uint32_t row = i / L, l = i - row * L;
@@ -63,10 +64,12 @@ void decompose_init_attributes() {
           "decompose smem");
 }
 
-void launch_decompose(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, cudaStream_t st) {
-    const uint32_t blocks = (d.N + kDecCoeffs - 1) / kDecCoeffs;
+void launch_decompose(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, uint32_t n_begin,
+                      uint32_t n_end, cudaStream_t st) {
+    if (n_end <= n_begin) return;
+    const uint32_t blocks = (n_end - n_begin + kDecCoeffs - 1) / kDecCoeffs;
     const size_t smem = kDecCoeffs * (static_cast<size_t>(d.L) + 1) * sizeof(uint32_t);
-    k_decompose_simt<<<blocks, kDecThreads, smem, st>>>(d, limbs, res, operand);
+    k_decompose_simt<<<blocks, kDecThreads, smem, st>>>(d, limbs, res, operand, n_begin, n_end);
 }
 
 }  // namespace fpm

@@ -70,15 +70,16 @@ __device__ __forceinline__ uint32_t fold49(uint64_t v, uint4 f) {
 }
 
 __global__ void __launch_bounds__(kThreads)
-    k_decompose_tc(DevPoint d, const uint32_t* __restrict__ limbs, uint32_t* __restrict__ res, int operand) {
+    k_decompose_tc(DevPoint d, const uint32_t* __restrict__ limbs, uint32_t* __restrict__ res, int operand,
+                   uint32_t n_begin, uint32_t n_end) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const uint32_t kb = d.dec_kb;          // GEMM K in bytes (4L rounded up to 32)
     const int nch = d.dec_chunks;
     const Smem sm = carve(smem_raw, kb);
     const uint8_t* img = operand ? d.dec_img_b : d.dec_img_a;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t n0 = blockIdx.x * kRows;
-    const uint32_t nk = min(kRows, d.N - n0);
+    const uint32_t n0 = n_begin + blockIdx.x * kRows;
+    const uint32_t nk = min(kRows, n_end - n0);
     const int L = d.L;
 
     if (threadIdx.x == 0) {
@@ -104,7 +105,11 @@ __global__ void __launch_bounds__(kThreads)
             __syncthreads();
         }
         const uint32_t total = nk * static_cast<uint32_t>(L);
-        const uint32_t n16 = total / 4;
+        // 16-byte loads need the caller's limbs 16-byte aligned (the block's
+        // start n0 L 4 is a multiple of 16 then); otherwise every word goes
+        // through the word-wise tail path below.
+        const bool vec = (reinterpret_cast<uintptr_t>(limbs) & 15u) == 0;
+        const uint32_t n16 = vec ? total / 4 : 0;
         const uint4* src4 = reinterpret_cast<const uint4*>(limbs + static_cast<size_t>(n0) * L);
         // w / L = mulhi(w, ceil(2^32 / L)) exactly for w < 2^16 (L = 1 divides trivially).
         const uint32_t inv_l = L == 1 ? 0u : 0xFFFFFFFFu / static_cast<uint32_t>(L) + 1;
@@ -136,7 +141,7 @@ __global__ void __launch_bounds__(kThreads)
             }
         }
         const uint32_t* src = limbs + static_cast<size_t>(n0) * L;
-        if (threadIdx.x < total - 4 * n16) place(4 * n16 + threadIdx.x, src[4 * n16 + threadIdx.x]);
+        for (uint32_t w = 4 * n16 + threadIdx.x; w < total; w += kThreads) place(w, src[w]);
     }
     tc::fence_proxy_async_smem();
     tc::tc_fence_before();
@@ -246,9 +251,11 @@ void decompose_tc_init_attributes() {
           "decompose_tc smem");
 }
 
-void launch_decompose_tc(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, cudaStream_t st) {
-    const uint32_t blocks = (d.N + kRows - 1) / kRows;
-    k_decompose_tc<<<blocks, kThreads, smem_bytes(d.dec_kb), st>>>(d, limbs, res, operand);
+void launch_decompose_tc(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, uint32_t n_begin,
+                         uint32_t n_end, cudaStream_t st) {
+    if (n_end <= n_begin) return;
+    const uint32_t blocks = (n_end - n_begin + kRows - 1) / kRows;
+    k_decompose_tc<<<blocks, kThreads, smem_bytes(d.dec_kb), st>>>(d, limbs, res, operand, n_begin, n_end);
 }
 
 }  // namespace fpm

@@ -8,6 +8,7 @@
 #include "engine.h"
 #include "kernels.h"
 
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -88,6 +89,7 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
         B_ = dalloc<uint32_t>(residues());
         check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
         check(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking), "stream");
+        check(cudaStreamCreateWithFlags(&out_, cudaStreamNonBlocking), "stream");
     } catch (...) {
         release();
         throw;
@@ -101,9 +103,12 @@ void Engine::release() {
     if (copy_) cudaStreamSynchronize(copy_);
     for (auto e : events_) cudaEventDestroy(e);
     events_.clear();
+    if (out_) cudaStreamSynchronize(out_);
     if (stream_) cudaStreamDestroy(stream_);
     if (copy_) cudaStreamDestroy(copy_);
-    stream_ = copy_ = nullptr;
+    if (out_) cudaStreamDestroy(out_);
+    stream_ = copy_ = out_ = nullptr;
+    pool_.reset();
     for (void* p : dmem_) cudaFree(p);
     dmem_.clear();
     for (uint32_t* h : {ha_, hb_, hc_}) {
@@ -112,19 +117,20 @@ void Engine::release() {
     ha_ = hb_ = hc_ = nullptr;
 }
 
-void Engine::launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, cudaStream_t st) {
+void Engine::launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, uint32_t n0, uint32_t n1,
+                        cudaStream_t st) {
     if (simt_) {
-        launch_decompose(dp_, d_limbs, d_res, operand, st);
+        launch_decompose(dp_, d_limbs, d_res, operand, n0, n1, st);
     } else {
-        launch_decompose_tc(dp_, d_limbs, d_res, operand, st);
+        launch_decompose_tc(dp_, d_limbs, d_res, operand, n0, n1, st);
     }
 }
 
-void Engine::launch_crt_any(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st) {
+void Engine::launch_crt_any(const uint32_t* d_y, uint32_t* d_c, uint32_t n0, uint32_t n1, cudaStream_t st) {
     if (simt_ || !crt_uses_tc(plan_)) {
-        launch_crt(dp_, d_y, d_c, st);
+        launch_crt(dp_, d_y, d_c, n0, n1, st);
     } else {
-        launch_crt_tc(dp_, d_y, d_c, st);
+        launch_crt_tc(dp_, d_y, d_c, n0, n1, st);
     }
 }
 
@@ -136,7 +142,7 @@ uint32_t Engine::take_error() {
 }
 
 void Engine::decompose(const uint32_t* d_limbs, uint32_t* d_res, int operand, cudaStream_t st) {
-    launch_dec(d_limbs, d_res, operand, st);
+    launch_dec(d_limbs, d_res, operand, 0, plan_.N, st);
     check(cudaGetLastError(), "decompose launch");
 }
 
@@ -146,39 +152,114 @@ void Engine::transform(uint32_t* d_A, uint32_t* d_B, int mode, cudaStream_t st) 
 }
 
 void Engine::crt(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st) {
-    launch_crt_any(d_y, d_c, st);
+    launch_crt_any(d_y, d_c, 0, plan_.N, st);
     check(cudaGetLastError(), "crt launch");
 }
 
 void Engine::run_device(const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t st) {
-    launch_dec(d_a, A_, 0, st);
-    launch_dec(d_b, B_, 1, st);
+    launch_dec(d_a, A_, 0, 0, plan_.N, st);
+    launch_dec(d_b, B_, 1, 0, plan_.N, st);
     launch_ntt(dp_, A_, B_, kRowProduct, st);
-    launch_crt_any(A_, d_c, st);
+    launch_crt_any(A_, d_c, 0, plan_.N, st);
     check(cudaGetLastError(), "product launch");
 }
 
-void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c) {
-    const size_t n = words(), bytes = n * sizeof(uint32_t);
-    if (!la_) {
-        la_ = dalloc<uint32_t>(n);
-        lb_ = dalloc<uint32_t>(n);
-        lc_ = dalloc<uint32_t>(n);
-        check(cudaHostAlloc(reinterpret_cast<void**>(&ha_), bytes, cudaHostAllocDefault), "pinned");
-        check(cudaHostAlloc(reinterpret_cast<void**>(&hb_), bytes, cudaHostAllocDefault), "pinned");
-        check(cudaHostAlloc(reinterpret_cast<void**>(&hc_), bytes, cudaHostAllocDefault), "pinned");
+namespace {
+
+bool is_pinned(const void* p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
     }
-    std::memcpy(ha_, a, bytes);
-    check(cudaMemcpyAsync(la_, ha_, bytes, cudaMemcpyHostToDevice, stream_), "copy a");
-    std::memcpy(hb_, b, bytes);
-    check(cudaMemcpyAsync(lb_, hb_, bytes, cudaMemcpyHostToDevice, stream_), "copy b");
-    run_device(la_, lb_, lc_, stream_);
-    check(cudaMemcpyAsync(hc_, lc_, bytes, cudaMemcpyDeviceToHost, stream_), "copy c");
-    check(cudaStreamSynchronize(stream_), "product");
+    return at.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+void Engine::ensure_host_path() {
+    if (la_) return;
+    const size_t n = words(), bytes = n * sizeof(uint32_t);
+    la_ = dalloc<uint32_t>(n);
+    lb_ = dalloc<uint32_t>(n);
+    lc_ = dalloc<uint32_t>(n);
+    check(cudaHostAlloc(reinterpret_cast<void**>(&ha_), bytes, cudaHostAllocDefault), "pinned");
+    check(cudaHostAlloc(reinterpret_cast<void**>(&hb_), bytes, cudaHostAllocDefault), "pinned");
+    check(cudaHostAlloc(reinterpret_cast<void**>(&hc_), bytes, cudaHostAllocDefault), "pinned");
+    // I/O chunks: FPM_IO_CHUNKS equal slices (default 4) on 128-coefficient
+    // boundaries, so a chunk's decompose and CRT blocks never straddle two.
+    int want = 4;
+    if (const char* v = std::getenv("FPM_IO_CHUNKS")) want = std::max(1, std::atoi(v));
+    const uint32_t N = plan_.N;
+    const uint32_t unit = 128;
+    const uint32_t units = (N + unit - 1) / unit;
+    const uint32_t nch = std::min<uint32_t>(static_cast<uint32_t>(want), units);
+    chunk_at_.clear();
+    for (uint32_t k = 0; k <= nch; ++k) chunk_at_.push_back(std::min(N, units * k / nch * unit));
+    events_.resize(4 * nch);
+    for (auto& e : events_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    pool_.reset(new CopyPool(default_copy_threads()));
+}
+
+void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* (*out_fn)(void*),
+                      void* out_arg) {
+    if (!c && !out_fn) throw std::runtime_error("run_host: no destination");
+    ensure_host_path();
+    const int L = plan_.L;
+    const size_t nch = chunk_at_.size() - 1;
+    const bool pin_a = is_pinned(a), pin_b = is_pinned(b), pin_c = c && is_pinned(c);
+    cudaEvent_t* in_ev = events_.data();              // 2 nch
+    cudaEvent_t* crt_ev = events_.data() + 2 * nch;   // nch
+    cudaEvent_t* out_ev = events_.data() + 3 * nch;   // nch
+
+    // In: per chunk, (stage,) DMA, then that chunk's decompose.
+    const uint32_t* src[2] = {a, b};
+    const bool pinned[2] = {pin_a, pin_b};
+    uint32_t* stage[2] = {ha_, hb_};
+    uint32_t* dlimbs[2] = {la_, lb_};
+    uint32_t* res[2] = {A_, B_};
+    for (int op = 0; op < 2; ++op) {
+        for (size_t k = 0; k < nch; ++k) {
+            const uint32_t n0 = chunk_at_[k], n1 = chunk_at_[k + 1];
+            const size_t off = static_cast<size_t>(n0) * L, bytes = static_cast<size_t>(n1 - n0) * L * 4;
+            const uint32_t* from = src[op] + off;
+            if (!pinned[op]) {
+                pool_->copy(stage[op] + off, from, bytes);
+                from = stage[op] + off;
+            }
+            check(cudaMemcpyAsync(dlimbs[op] + off, from, bytes, cudaMemcpyHostToDevice, copy_), "copy in");
+            check(cudaEventRecord(in_ev[op * nch + k], copy_), "event");
+            check(cudaStreamWaitEvent(stream_, in_ev[op * nch + k], 0), "wait");
+            launch_dec(dlimbs[op], res[op], op, n0, n1, stream_);
+        }
+    }
+    launch_ntt(dp_, A_, B_, kRowProduct, stream_);
+    // Out: per chunk, the CRT, then its DMA (to c itself when c is pinned).
+    uint32_t* dst = pin_c ? c : hc_;
+    for (size_t k = 0; k < nch; ++k) {
+        const uint32_t n0 = chunk_at_[k], n1 = chunk_at_[k + 1];
+        const size_t off = static_cast<size_t>(n0) * L, bytes = static_cast<size_t>(n1 - n0) * L * 4;
+        launch_crt_any(A_, lc_, n0, n1, stream_);
+        check(cudaEventRecord(crt_ev[k], stream_), "event");
+        check(cudaStreamWaitEvent(out_, crt_ev[k], 0), "wait");
+        check(cudaMemcpyAsync(dst + off, lc_ + off, bytes, cudaMemcpyDeviceToHost, out_), "copy out");
+        check(cudaEventRecord(out_ev[k], out_), "event");
+    }
+    check(cudaGetLastError(), "product launch");
+    if (!c) c = out_fn(out_arg);
+    if (!pin_c) {
+        for (size_t k = 0; k < nch; ++k) {
+            const uint32_t n0 = chunk_at_[k], n1 = chunk_at_[k + 1];
+            const size_t off = static_cast<size_t>(n0) * L, bytes = static_cast<size_t>(n1 - n0) * L * 4;
+            check(cudaEventSynchronize(out_ev[k]), "copy out");
+            pool_->copy(c + off, hc_ + off, bytes);
+        }
+    } else {
+        check(cudaEventSynchronize(out_ev[nch - 1]), "copy out");
+    }
     if (const uint32_t e = take_error()) {
         throw std::runtime_error("a kernel pipeline wait timed out (error word " + std::to_string(e) + ")");
     }
-    std::memcpy(c, hc_, bytes);
 }
 
 }  // namespace fpm

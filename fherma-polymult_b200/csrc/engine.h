@@ -2,12 +2,14 @@
 // residue workspaces, pinned staging and the launch sequence of a product.
 #pragma once
 
+#include "copy_pool.h"
 #include "device.cuh"
 #include "plan.h"
 
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <vector>
 
 namespace fpm {
@@ -28,9 +30,16 @@ public:
     // residue workspaces are used, so calls on one engine must not overlap.
     void run_device(const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t st);
 
-    // c = a b on host buffers (pageable or not, N x L each); returns when c is
-    // written.
-    void run_host(const uint32_t* a, const uint32_t* b, uint32_t* c);
+    // c = a b on host buffers (N x L each); returns when c is written.  Pinned
+    // buffers are read and written by DMA directly; pageable ones are staged
+    // through pinned memory by the copy pool.  Either way the operands move in
+    // chunks, each chunk's decompose starting as soon as it has landed, and the
+    // result moves out chunk by chunk behind the CRT.  With c == nullptr the
+    // destination comes from out_fn(out_arg), called on this thread once the
+    // whole product is enqueued and right before c is first written, so a
+    // caller can allocate c while the GPU works.
+    void run_host(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* (*out_fn)(void*) = nullptr,
+                  void* out_arg = nullptr);
 
     // Stages, for checks against the oracle.
     void decompose(const uint32_t* d_limbs, uint32_t* d_res, int operand, cudaStream_t st);
@@ -46,8 +55,10 @@ public:
 
 private:
     void release();
-    void launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, cudaStream_t st);
-    void launch_crt_any(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st);
+    void launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, uint32_t n0, uint32_t n1,
+                    cudaStream_t st);
+    void launch_crt_any(const uint32_t* d_y, uint32_t* d_c, uint32_t n0, uint32_t n1, cudaStream_t st);
+    void ensure_host_path();
     template <class T>
     T* dalloc(size_t count);
     template <class T>
@@ -66,9 +77,12 @@ private:
     uint32_t* ha_ = nullptr;  // pinned staging
     uint32_t* hb_ = nullptr;
     uint32_t* hc_ = nullptr;
-    cudaStream_t stream_ = nullptr;
-    cudaStream_t copy_ = nullptr;
+    cudaStream_t stream_ = nullptr;   // kernels
+    cudaStream_t copy_ = nullptr;     // host -> device
+    cudaStream_t out_ = nullptr;      // device -> host
     std::vector<cudaEvent_t> events_;
+    std::vector<uint32_t> chunk_at_;  // I/O chunk boundaries (coefficients)
+    std::unique_ptr<CopyPool> pool_;
 };
 
 // Shared-memory opt-ins, once per device per process.

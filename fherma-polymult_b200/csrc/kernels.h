@@ -39,17 +39,22 @@ void crt_tc_init_attributes();
 
 // limbs (N x L, coefficient-major) -> residues (K x N); operand 1 (b) is
 // scaled for the pointwise step.
-void launch_decompose(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, cudaStream_t st);
+// Coefficients [n_begin, n_end) only (multiples of 128 but for the end).
+void launch_decompose(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, uint32_t n_begin,
+                      uint32_t n_end, cudaStream_t st);
 
 // Residues A, B -> y_j in A (mode kRowProduct), or the forward transforms of
 // both in place (mode kRowForward).
 void launch_ntt(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStream_t st);
 
 // The same on the tensor cores.
-void launch_decompose_tc(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, cudaStream_t st);
+void launch_decompose_tc(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, uint32_t n_begin,
+                         uint32_t n_end, cudaStream_t st);
 
 // y_j (K x N) -> c (N x L) mod q: CUDA cores, and tensor cores (L >= 2).
-void launch_crt(const DevPoint& d, const uint32_t* Y, uint32_t* c, cudaStream_t st);
-void launch_crt_tc(const DevPoint& d, const uint32_t* Y, uint32_t* c, cudaStream_t st);
+void launch_crt(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_begin, uint32_t n_end,
+                cudaStream_t st);
+void launch_crt_tc(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_begin, uint32_t n_end,
+                   cudaStream_t st);
 
 }  // namespace fpm

@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(kNttThreads, 5) k_ntt_row(DevPoint d, uint32_t
 // thread per stage, full twiddle tables from global memory, full reduction.
 
 __global__ void __launch_bounds__(kNttThreads) k_ntt_small(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
-    extern __shared__ __align__(16) uint32_t smem[];
+    extern __shared__ __align__(1024) uint32_t smem[];
     const uint32_t N = d.N, logN = d.logN;
     uint32_t* ta = smem;
     uint32_t* tb = smem + N;
