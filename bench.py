@@ -1,5 +1,5 @@
 """Benchmark: µs per exact negacyclic product at N = 65536, W = 2048 (q a seeded
-random odd 2048-bit modulus, 64 limbs, K = 134 primes), on one or more B200s.
+random odd 2048-bit modulus, 64 limbs, K = 139 primes below 2^30), on one or more B200s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload N65536_W2048|N65536_W1747|N32768_W868|N4096_W256]
@@ -247,6 +247,12 @@ def main():
     ctx.stage_decompose(db.data_ptr(), B.data_ptr(), 1, sp)
     stages["transform"] = time_stage(lambda: ctx.stage_transform(A.data_ptr(), B.data_ptr(), 0, sp))
     stages["crt"] = time_stage(lambda: ctx.stage_crt(A.data_ptr(), dc.data_ptr(), sp))
+    # One kernel at a time (the transform's passes alone: modes 2, 3, 4).
+    kernels = {"k_decompose_tc": stages["decompose"], "k_crt_tc": stages["crt"]}
+    if ctx.info.logR:
+        kernels["k_ntt_col_fwd"] = time_stage(lambda: ctx.stage_transform(A.data_ptr(), B.data_ptr(), 2, sp))
+        kernels["k_ntt_col_inv"] = time_stage(lambda: ctx.stage_transform(A.data_ptr(), B.data_ptr(), 4, sp))
+    kernels["k_ntt_row"] = time_stage(lambda: ctx.stage_transform(A.data_ptr(), B.data_ptr(), 3, sp))
 
     # Timed region.
     if world > 1:
@@ -300,10 +306,20 @@ def main():
 
     hbm, peak_kind = peaks()
     ab = algorithmic_bytes(N, L, K)
-    stage_bytes = {"decompose": ab["decompose"], "transform": ab["ntt_col_fwd"] + ab["ntt_row"] + ab["ntt_col_inv"],
-                   "crt": ab["crt"]}
-    dom = max(stages, key=stages.get)
-    achieved = stage_bytes[dom] / (stages[dom] * 1e-6) / 1e9
+    kernel_bytes = {"k_decompose_tc": ab["decompose"], "k_ntt_col_fwd": ab["ntt_col_fwd"], "k_ntt_row": ab["ntt_row"],
+                    "k_ntt_col_inv": ab["ntt_col_inv"], "k_crt_tc": ab["crt"]}
+    # launches per product: the dominant kernel's time share in one product
+    per_product = {"k_decompose_tc": 2, "k_ntt_col_fwd": 1, "k_ntt_row": 1, "k_ntt_col_inv": 1, "k_crt_tc": 1}
+    dom = max(kernels, key=lambda k: kernels[k] * per_product[k])
+    achieved = kernel_bytes[dom] / (kernels[dom] * 1e-6) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tr = json.load(f)
+        entry = tr.get(args.workload, {}).get(dom)
+        if entry:
+            traffic = entry["dram_bytes_per_launch"]
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -344,9 +360,12 @@ def main():
             "e2e_pageable": {"value": e2e_pageable_us, "unit": "us/product",
                              "host_buffers": "pageable numpy (fpm_run stages through pinned memory)"},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
-                         "algorithmic_bytes": stage_bytes[dom]},
+                         "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes": kernel_bytes[dom],
+                         "note": "algorithmic bytes per launch / CUDA-event launch time; traffic = ncu dram "
+                                 "read+write per launch from profiles/ncu_traffic.json"},
             "stages_us": stages,
+            "kernels_us": kernels,
             "product_algorithmic_bytes": ab["product"],
             "product_hbm_frac": ab["product"] / (us_per_product * world * 1e-6) / 1e9 / hbm,
             "gpu_launches": args.steps * launches_per_product,

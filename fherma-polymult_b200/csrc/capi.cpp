@@ -151,7 +151,7 @@ int fpm_stage_decompose(fpm_ctx* ctx, const uint32_t* d_limbs, uint32_t* d_res, 
 }
 
 int fpm_stage_transform(fpm_ctx* ctx, uint32_t* d_A, uint32_t* d_B, int mode, void* stream) {
-    if (!ctx || !d_A || !d_B || (mode != 0 && mode != 1))
+    if (!ctx || !d_A || !d_B || mode < 0 || mode > 4)
         return fail(FPM_EINVAL, "fpm_stage_transform: bad argument");
     return guarded([&] { ctx->engine->transform(d_A, d_B, mode, as_stream(stream)); });
 }

@@ -45,6 +45,10 @@ struct DevPoint {
 enum RowMode : int {
     kRowProduct = 0,   // forward rows of A and B, pointwise A B, inverse rows -> A
     kRowForward = 1,   // forward rows of A and B only (for stage checks)
+    // single launches of the four-step chain, for timing one kernel at a time
+    kPassColFwd = 2,
+    kPassRow = 3,
+    kPassColInv = 4,
 };
 
 }  // namespace fpm

@@ -449,7 +449,11 @@ void launch_row_t(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStr
 
 template <bool LAZY>
 void launch_ntt_t(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStream_t st) {
-    switch (d.logR) {
+    const bool col_fwd = mode == kRowProduct || mode == kRowForward || mode == kPassColFwd;
+    const bool row = mode == kRowProduct || mode == kRowForward || mode == kPassRow;
+    const bool col_inv = mode == kRowProduct || mode == kPassColInv;
+    const int row_mode = mode == kRowForward ? kRowForward : kRowProduct;
+    if (col_fwd) switch (d.logR) {
         case 0: break;
         case 6: launch_col_fwd_t<6, LAZY>(d, A, B, st); break;
         case 7: launch_col_fwd_t<7, LAZY>(d, A, B, st); break;
@@ -459,17 +463,16 @@ void launch_ntt_t(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStr
         case 11: launch_col_fwd_t<11, LAZY>(d, A, B, st); break;
         default: throw std::runtime_error("unsupported column length");
     }
-    switch (d.logS) {
-        case 6: launch_row_t<6, LAZY>(d, A, B, mode, st); break;
-        case 7: launch_row_t<7, LAZY>(d, A, B, mode, st); break;
-        case 8: launch_row_t<8, LAZY>(d, A, B, mode, st); break;
-        case 9: launch_row_t<9, LAZY>(d, A, B, mode, st); break;
-        case 10: launch_row_t<10, LAZY>(d, A, B, mode, st); break;
-        case 11: launch_row_t<11, LAZY>(d, A, B, mode, st); break;
+    if (row) switch (d.logS) {
+        case 6: launch_row_t<6, LAZY>(d, A, B, row_mode, st); break;
+        case 7: launch_row_t<7, LAZY>(d, A, B, row_mode, st); break;
+        case 8: launch_row_t<8, LAZY>(d, A, B, row_mode, st); break;
+        case 9: launch_row_t<9, LAZY>(d, A, B, row_mode, st); break;
+        case 10: launch_row_t<10, LAZY>(d, A, B, row_mode, st); break;
+        case 11: launch_row_t<11, LAZY>(d, A, B, row_mode, st); break;
         default: throw std::runtime_error("unsupported row length");
     }
-    if (mode == kRowForward) return;
-    switch (d.logR) {
+    if (col_inv) switch (d.logR) {
         case 0: break;
         case 6: launch_col_inv_t<6, LAZY>(d, A, st); break;
         case 7: launch_col_inv_t<7, LAZY>(d, A, st); break;
@@ -495,7 +498,10 @@ void ntt_init_attributes() {
 // canonical).
 void launch_ntt(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStream_t st) {
     if (d.logN <= kSmallLogN) {
-        k_ntt_small<<<d.K, kNttThreads, 2 * d.N * sizeof(uint32_t), st>>>(d, A, B, mode);
+        if (mode == kRowProduct || mode == kRowForward || mode == kPassRow)
+            k_ntt_small<<<d.K, kNttThreads, 2 * d.N * sizeof(uint32_t), st>>>(d, A, B,
+                                                                                mode == kRowForward ? kRowForward
+                                                                                                    : kRowProduct);
         return;
     }
     if (d.lazy) {

@@ -103,6 +103,8 @@ FPM_API int fpm_get_primes(const fpm_ctx* ctx, uint32_t* out);
  *   crt:       y (K x N) -> c (N x L) mod q (reference k_crt, solve.cu:264-277). */
 FPM_API int fpm_stage_decompose(fpm_ctx* ctx, const uint32_t* d_limbs, uint32_t* d_res, int operand, void* stream);
 FPM_API int fpm_stage_transform(fpm_ctx* ctx, uint32_t* d_A, uint32_t* d_B, int mode, void* stream);
+/* Modes 2, 3, 4 of fpm_stage_transform launch one kernel of the chain alone
+ * (forward column pass, fused row pass, inverse column pass), for timing. */
 FPM_API int fpm_stage_crt(fpm_ctx* ctx, const uint32_t* d_y, uint32_t* d_c, void* stream);
 
 #ifdef __cplusplus
