@@ -107,6 +107,11 @@ int fpm_run_device(fpm_ctx* ctx, const uint32_t* d_a, const uint32_t* d_b, uint3
     return guarded([&] { ctx->engine->run_device(d_a, d_b, d_c, as_stream(stream)); });
 }
 
+int fpm_run_device_noalloc(fpm_ctx* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, void* stream) {
+    if (!ctx || !d_a || !d_b || !d_c) return fail(FPM_EINVAL, "fpm_run_device_noalloc: NULL argument");
+    return guarded([&] { ctx->engine->run_device_static(d_a, d_b, d_c, as_stream(stream)); });
+}
+
 void fpm_free(fpm_ctx* ctx) {
     if (!ctx) return;
     delete ctx->engine;

@@ -30,6 +30,13 @@ public:
     // residue workspaces are used, so calls on one engine must not overlap.
     void run_device(const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t st);
 
+    // As run_device, but the residue workspaces and the error word come from a
+    // static device array of static_scratch_bytes() (static_scratch.cu), not
+    // from this engine; allocates nothing.  Throws std::runtime_error when the
+    // point's scratch does not fit or another device is current.
+    void run_device_static(const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t st);
+    size_t static_scratch_words_needed() const;
+
     // c = a b on host buffers (N x L each); returns when c is written.  Pinned
     // buffers are read and written by DMA directly; pageable ones are staged
     // through pinned memory by the copy pool.  Either way the operands move in
@@ -54,6 +61,7 @@ public:
     size_t residues() const { return static_cast<size_t>(plan_.K) * plan_.N; }
 
 private:
+    size_t static_scratch_err_offset() const;
     void release();
     void launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, uint32_t n0, uint32_t n1,
                     cudaStream_t st);
@@ -87,5 +95,8 @@ private:
 
 // Shared-memory opt-ins, once per device per process.
 void ensure_kernel_attributes(int device);
+
+// Size of the static scratch array behind Engine::run_device_static.
+size_t static_scratch_bytes();
 
 }  // namespace fpm

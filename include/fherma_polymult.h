@@ -73,6 +73,23 @@ FPM_API int fpm_run(fpm_ctx* ctx, const uint32_t* a, const uint32_t* b, uint32_t
  * Calls on one context must be ordered on one stream (they share workspaces). */
 FPM_API int fpm_run_device(fpm_ctx* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, void* stream);
 
+/* No counterpart in the reference.  For callers that cannot allocate device
+ * memory once they are running -- a process held to a fixed device-memory
+ * budget, or a caller issuing work where cudaMalloc is not allowed -- this is
+ * fpm_run_device with the product's scratch (the two K x N residue workspaces
+ * and the error word) in one static device array of 80 MiB that every GPU
+ * loading the library holds until the process exits; the call itself
+ * allocates nothing.  The caller passes a context from fpm_init (made on the
+ * current device) and the device buffers a, b, c (N x L u32 each).  A point
+ * needing more than 80 MiB of scratch (2 K N words: every point up to
+ * N = 65536 at W = 2048 fits) returns FPM_EINVAL with a message naming both
+ * sizes.  The first call on each device looks up the array's address and
+ * loads its module: make it before any stream capture.  All calls, from every
+ * context, share the one array: calls whose work overlaps on the GPU race, so
+ * order them on one stream. */
+FPM_API int fpm_run_device_noalloc(fpm_ctx* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,
+                                   void* stream);
+
 /* Replaces fherma_free (reference fherma.h:48, solve.cu:1061-1083); accepts
  * NULL. */
 FPM_API void fpm_free(fpm_ctx* ctx);
