@@ -1,0 +1,421 @@
+// Batched products: grouped launches captured as one CUDA graph (batch.h).
+#include "batch.h"
+#include "kernels.h"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <stdexcept>
+#include <tuple>
+
+namespace fpm {
+
+namespace {
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Fills GroupTables item by item and launches each when it is full.
+struct TableFill {
+    std::unique_ptr<GroupTable> t{new GroupTable};
+    TableFill() { reset(); }
+    void reset() {
+        std::memset(t.get(), 0, sizeof(GroupTable));
+    }
+    bool full() const { return t->count == static_cast<uint32_t>(kGroupMax); }
+    void add(const DevPoint& d, uint32_t* a, uint32_t* b, uint32_t* A, uint32_t* B, uint32_t* c, uint32_t j0,
+             uint32_t blocks) {
+        GroupItem& it = t->item[t->count];
+        it.d = d;
+        it.a = a;
+        it.b = b;
+        it.A = A;
+        it.B = B;
+        it.c = c;
+        it.j0 = j0;
+        t->total += blocks;
+        t->count += 1;
+        t->first[t->count] = t->total;
+    }
+};
+
+struct TransformClass {
+    uint32_t logR, logS;
+    bool lazy;
+    bool operator<(const TransformClass& o) const {
+        return std::tie(logR, logS, lazy) < std::tie(o.logR, o.logS, o.lazy);
+    }
+};
+
+}  // namespace
+
+Batch::Batch(const std::vector<Engine*>& engines) {
+    if (engines.empty()) throw std::runtime_error("batch: no products");
+    int dev = -1;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    size_t bytes = 0;
+    for (Engine* e : engines) {
+        if (!e) throw std::runtime_error("batch: null context");
+        if (e->device() != dev) throw std::runtime_error("batch: every context must live on the current device");
+        bytes += 3 * align256(e->words() * 4) + 2 * align256(e->residues() * 4);
+    }
+    bytes += 256;   // error word
+    try {
+        check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev), "SM count");
+        check(cudaMalloc(&slab_, bytes), "cudaMalloc (batch)");
+        slab_bytes_ = bytes;
+        check(cudaMemset(slab_, 0, bytes), "memset (batch)");
+        uint8_t* at = static_cast<uint8_t*>(slab_);
+        auto take = [&](size_t n) {
+            uint32_t* p = reinterpret_cast<uint32_t*>(at);
+            at += align256(n * 4);
+            return p;
+        };
+        err_ = take(1);
+        for (Engine* e : engines) {
+            Prod p{};
+            p.e = e;
+            p.d = e->point();
+            p.d.err = err_;
+            p.a = take(e->words());
+            p.b = take(e->words());
+            p.c = take(e->words());
+            p.A = take(e->residues());
+            p.B = take(e->residues());
+            const HostPlan& pl = e->plan();
+            p.cost = static_cast<double>(pl.K) * pl.N * (pl.g.logN + 0.5 * pl.L);
+            prods_.push_back(p);
+        }
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+        build_graph();
+    } catch (...) {
+        release_graph();
+        for (auto s : branches_) cudaStreamDestroy(s);
+        for (auto ev : events_) cudaEventDestroy(ev);
+        if (stream_) cudaStreamDestroy(stream_);
+        if (slab_) cudaFree(slab_);
+        throw;
+    }
+}
+
+Batch::~Batch() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    release_graph();
+    for (auto s : branches_) cudaStreamDestroy(s);
+    for (auto ev : events_) cudaEventDestroy(ev);
+    if (stream_) cudaStreamDestroy(stream_);
+    if (slab_) cudaFree(slab_);
+}
+
+void Batch::release_graph() {
+    if (exec_) cudaGraphExecDestroy(exec_);
+    exec_ = nullptr;
+}
+
+uint64_t Batch::occupancy_key(int pass, uint32_t logR, uint32_t logS, bool lazy) {
+    return (static_cast<uint64_t>(pass) << 32) | (logR << 16) | (logS << 1) | (lazy ? 1u : 0u);
+}
+
+cudaStream_t Batch::branch(size_t i) {
+    while (branches_.size() <= i) {
+        cudaStream_t s = nullptr;
+        check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+        branches_.push_back(s);
+    }
+    return branches_[i];
+}
+
+void Batch::set_schedule(const BatchSchedule& s) {
+    if (s.layout < 0 || s.layout > 2 || s.order < 0 || s.order > 1 || s.prime_group < 0 || s.grid < 0)
+        throw std::runtime_error("batch: invalid schedule");
+    sched_ = s;
+    build_graph();
+}
+
+void Batch::build_graph() {
+    check(cudaStreamSynchronize(stream_), "batch sync");
+    release_graph();
+    // Events and branch streams used by the capture, created outside it.
+    const size_t need = 2 * (prods_.size() + 8);
+    while (events_.size() < need) {
+        cudaEvent_t ev = nullptr;
+        check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+        events_.push_back(ev);
+    }
+    // One branch stream per transform geometry, and the resident blocks per SM
+    // of every grouped transform kernel (persistent grids).
+    size_t classes = 0;
+    std::vector<uint32_t> seen;
+    for (const Prod& p : prods_) {
+        if (p.d.logN <= kSmallLogN) continue;
+        const uint32_t key = p.d.logR * 64 + p.d.logS * 2 + (p.d.lazy ? 1 : 0);
+        if (std::find(seen.begin(), seen.end(), key) != seen.end()) continue;
+        seen.push_back(key);
+        ++classes;
+        for (int pass : {int(kPassColFwd), int(kPassRow), int(kPassColInv)}) {
+            if (pass != kPassRow && p.d.logR == 0) continue;
+            const uint64_t k = occupancy_key(pass, p.d.logR, p.d.logS, p.d.lazy != 0);
+            if (!occupancy_.count(k)) occupancy_[k] = ntt_group_occupancy(pass, p.d.logR, p.d.logS, p.d.lazy != 0);
+        }
+    }
+    for (size_t i = 0; i < classes; ++i) branch(i);
+    cudaGraph_t graph = nullptr;
+    check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+        enqueue(stream_);
+    } catch (...) {
+        cudaStreamEndCapture(stream_, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        throw;
+    }
+    check(cudaStreamEndCapture(stream_, &graph), "end capture");
+    const cudaError_t e = cudaGraphInstantiate(&exec_, graph, 0);
+    cudaGraphDestroy(graph);
+    check(e, "graph instantiate");
+}
+
+void Batch::enqueue(cudaStream_t st) {
+    launches_ = 0;
+    std::vector<size_t> ord(prods_.size());
+    std::iota(ord.begin(), ord.end(), size_t(0));
+    if (sched_.order == 1) {
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return prods_[x].cost > prods_[y].cost; });
+    }
+    // Products by transform geometry; N <= 1024 runs the one-block-per-prime
+    // kernel, product by product.
+    std::map<TransformClass, std::vector<size_t>> classes;
+    std::vector<size_t> small;
+    for (size_t i : ord) {
+        const DevPoint& d = prods_[i].d;
+        if (d.logN <= kSmallLogN) {
+            small.push_back(i);
+        } else {
+            classes[TransformClass{d.logR, d.logS, d.lazy != 0}].push_back(i);
+        }
+    }
+    TableFill fill;
+
+    auto decompose = [&](const std::vector<size_t>& list, cudaStream_t s) {
+        fill.reset();
+        auto flush = [&] {
+            if (fill.t->count) {
+                launch_decompose_tc_group(*fill.t, s);
+                ++launches_;
+            }
+            fill.reset();
+        };
+        for (size_t i : list) {
+            const Prod& p = prods_[i];
+            if (p.e->simt()) {
+                launch_decompose(p.d, p.a, p.A, 0, 0, p.d.N, s);
+                launch_decompose(p.d, p.b, p.B, 1, 0, p.d.N, s);
+                launches_ += 2;
+                continue;
+            }
+            if (fill.full()) flush();
+            fill.add(p.d, p.a, p.b, p.A, p.B, p.c, 0, decompose_tc_group_blocks(p.d.N));
+        }
+        flush();
+    };
+    auto crt = [&](const std::vector<size_t>& list, cudaStream_t s) {
+        fill.reset();
+        auto flush = [&] {
+            if (fill.t->count) {
+                launch_crt_tc_group(*fill.t, s);
+                ++launches_;
+            }
+            fill.reset();
+        };
+        for (size_t i : list) {
+            const Prod& p = prods_[i];
+            if (p.e->simt() || !crt_uses_tc(p.e->plan())) {
+                launch_crt(p.d, p.A, p.c, 0, p.d.N, s);
+                ++launches_;
+                continue;
+            }
+            if (fill.full()) flush();
+            fill.add(p.d, p.a, p.b, p.A, p.B, p.c, 0, crt_tc_group_blocks(p.d.N));
+        }
+        flush();
+    };
+    auto small_ntt = [&](const std::vector<size_t>& list, cudaStream_t s) {
+        for (size_t i : list) {
+            launch_ntt(prods_[i].d, prods_[i].A, prods_[i].B, kRowProduct, s);
+            ++launches_;
+        }
+    };
+    // One geometry's chain: every item (a group of one product's primes)
+    // through the column pass, the fused row pass, the inverse column pass.
+    auto transform = [&](const TransformClass& g, const std::vector<size_t>& list, cudaStream_t s) {
+        struct Item {
+            size_t p;
+            uint32_t j0, nj;
+        };
+        std::vector<Item> items;
+        if (sched_.prime_group <= 0) {
+            for (size_t i : list) items.push_back({i, 0, static_cast<uint32_t>(prods_[i].d.K)});
+        } else {
+            // Round robin over the products, prime group by prime group.
+            const uint32_t grp = static_cast<uint32_t>(sched_.prime_group);
+            for (uint32_t r = 0;; ++r) {
+                bool any = false;
+                for (size_t i : list) {
+                    const uint32_t K = static_cast<uint32_t>(prods_[i].d.K), j0 = r * grp;
+                    if (j0 >= K) continue;
+                    items.push_back({i, j0, std::min(grp, K - j0)});
+                    any = true;
+                }
+                if (!any) break;
+            }
+        }
+        for (int pass : {int(kPassColFwd), int(kPassRow), int(kPassColInv)}) {
+            if (pass != kPassRow && g.logR == 0) continue;
+            const uint32_t per = ntt_blocks_per_prime(pass, g.logR, g.logS);
+            uint32_t grid = 0;
+            if (sched_.grid > 0) {
+                grid = static_cast<uint32_t>(sched_.grid) * static_cast<uint32_t>(sms_) *
+                       static_cast<uint32_t>(std::max(1, occupancy_.at(occupancy_key(pass, g.logR, g.logS, g.lazy))));
+            }
+            fill.reset();
+            auto flush = [&] {
+                if (fill.t->count) {
+                    launch_ntt_group(*fill.t, pass, g.logR, g.logS, g.lazy, grid, s);
+                    ++launches_;
+                }
+                fill.reset();
+            };
+            for (const Item& it : items) {
+                if (fill.full()) flush();
+                const Prod& p = prods_[it.p];
+                fill.add(p.d, p.a, p.b, p.A, p.B, p.c, it.j0, it.nj * per);
+            }
+            flush();
+        }
+    };
+
+    size_t ev = 0;
+    auto fork = [&](cudaStream_t from, cudaStream_t to) {
+        check(cudaEventRecord(events_.at(ev), from), "event record");
+        check(cudaStreamWaitEvent(to, events_.at(ev), 0), "stream wait");
+        ++ev;
+    };
+    std::vector<size_t> all(ord);
+    if (sched_.layout == 0) {
+        decompose(all, st);
+        for (auto& kv : classes) transform(kv.first, kv.second, st);
+        small_ntt(small, st);
+        crt(all, st);
+    } else if (sched_.layout == 1) {
+        decompose(all, st);
+        size_t b = 0;
+        std::vector<cudaStream_t> used;
+        for (auto& kv : classes) {
+            cudaStream_t s = branch(b++);
+            fork(st, s);
+            transform(kv.first, kv.second, s);
+            used.push_back(s);
+        }
+        small_ntt(small, st);
+        for (cudaStream_t s : used) fork(s, st);
+        crt(all, st);
+    } else {
+        size_t b = 0;
+        std::vector<cudaStream_t> used;
+        for (auto& kv : classes) {
+            cudaStream_t s = branch(b++);
+            fork(st, s);
+            decompose(kv.second, s);
+            transform(kv.first, kv.second, s);
+            crt(kv.second, s);
+            used.push_back(s);
+        }
+        decompose(small, st);
+        small_ntt(small, st);
+        crt(small, st);
+        for (cudaStream_t s : used) fork(s, st);
+    }
+    check(cudaGetLastError(), "batch launch");
+}
+
+void Batch::run_device(cudaStream_t st) { check(cudaGraphLaunch(exec_, st), "graph launch"); }
+
+void Batch::run_host(const uint32_t* const* a, const uint32_t* const* b, uint32_t* const* c) {
+    for (size_t i = 0; i < prods_.size(); ++i) {
+        const size_t bytes = prods_[i].e->words() * 4;
+        check(cudaMemcpyAsync(prods_[i].a, a[i], bytes, cudaMemcpyHostToDevice, stream_), "copy a");
+        check(cudaMemcpyAsync(prods_[i].b, b[i], bytes, cudaMemcpyHostToDevice, stream_), "copy b");
+    }
+    run_device(stream_);
+    for (size_t i = 0; i < prods_.size(); ++i) {
+        const size_t bytes = prods_[i].e->words() * 4;
+        check(cudaMemcpyAsync(c[i], prods_[i].c, bytes, cudaMemcpyDeviceToHost, stream_), "copy c");
+    }
+    check(cudaStreamSynchronize(stream_), "batch sync");
+    if (take_error()) throw std::runtime_error("batch: a tensor-core pipeline wait timed out");
+}
+
+uint32_t Batch::take_error() {
+    uint32_t e = 0;
+    check(cudaMemcpy(&e, err_, sizeof(e), cudaMemcpyDeviceToHost), "read error word");
+    if (e) check(cudaMemset(err_, 0, sizeof(e)), "clear error word");
+    return e;
+}
+
+double Batch::tune(int reps) {
+    if (reps < 1) reps = 1;
+    std::vector<BatchSchedule> cands;
+    for (int layout : {0, 1, 2})
+        for (int grp : {0, 16})
+            for (int grid : {0, 1}) cands.push_back(BatchSchedule{layout, 1, grp, grid});
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    check(cudaEventCreate(&t0), "event");
+    check(cudaEventCreate(&t1), "event");
+    auto time_current = [&]() {
+        run_device(stream_);   // warm-up
+        float best = 1e30f;
+        for (int r = 0; r < reps; ++r) {
+            check(cudaEventRecord(t0, stream_), "event");
+            run_device(stream_);
+            check(cudaEventRecord(t1, stream_), "event");
+            check(cudaEventSynchronize(t1), "event sync");
+            float ms = 0;
+            check(cudaEventElapsedTime(&ms, t0, t1), "elapsed");
+            best = std::min(best, ms);
+        }
+        return best;
+    };
+    BatchSchedule best_s = sched_;
+    float best = 1e30f;
+    try {
+        for (const BatchSchedule& s : cands) {
+            set_schedule(s);
+            const float ms = time_current();
+            if (ms < best) {
+                best = ms;
+                best_s = s;
+            }
+        }
+        // The given order against the best schedule found.
+        BatchSchedule s = best_s;
+        s.order = 0;
+        set_schedule(s);
+        const float ms = time_current();
+        if (ms < best) {
+            best = ms;
+            best_s = s;
+        }
+        set_schedule(best_s);
+    } catch (...) {
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        throw;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    if (take_error()) throw std::runtime_error("batch: a tensor-core pipeline wait timed out while tuning");
+    return best * 1000.0;
+}
+
+}  // namespace fpm

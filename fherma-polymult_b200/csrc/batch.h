@@ -1,0 +1,100 @@
+// Batched products: many points of uneven N and q width in one graph of
+// grouped launches.
+//
+// Each product keeps its own resident plan (an Engine from fpm_init).  The
+// batch owns one device slab with every product's operands, result and residue
+// workspaces, so its launch graph is fixed: one grouped decompose launch for
+// all products, per transform geometry (logR, logS) a grouped column / row /
+// inverse-column chain whose items are groups of a product's primes, and one
+// grouped CRT launch, all captured once as a CUDA graph and replayed.
+//
+// The schedule -- whether the geometry chains run as parallel graph branches,
+// the order of the items, how many primes one transform item carries, and
+// whether the transform grids are persistent -- is chosen by Batch::tune,
+// which times every candidate on this batch and keeps the fastest.
+#pragma once
+
+#include "engine.h"
+#include "group.cuh"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <vector>
+
+namespace fpm {
+
+struct BatchSchedule {
+    int layout = 1;        // 0 one stream; 1 geometry chains as branches between the shared
+                           // decompose and CRT; 2 a whole branch (decompose .. CRT) per geometry
+    int order = 1;         // 0 products as given; 1 largest first
+    int prime_group = 0;   // primes per transform item; 0 = all of a product's primes
+    int grid = 0;          // transform grids: 0 one block per tile; k > 0 persistent,
+                           // k x (resident blocks per SM) x SMs
+};
+
+class Batch {
+public:
+    // All engines on the current device; the batch does not own them, and
+    // they must outlive it.
+    explicit Batch(const std::vector<Engine*>& engines);
+    ~Batch();
+    Batch(const Batch&) = delete;
+    Batch& operator=(const Batch&) = delete;
+
+    size_t size() const { return prods_.size(); }
+    // Device limbs of product i (N_i x L_i u32 each): write a and b, read c.
+    uint32_t* a(size_t i) const { return prods_.at(i).a; }
+    uint32_t* b(size_t i) const { return prods_.at(i).b; }
+    uint32_t* c(size_t i) const { return prods_.at(i).c; }
+    size_t device_bytes() const { return slab_bytes_; }
+
+    const BatchSchedule& schedule() const { return sched_; }
+    void set_schedule(const BatchSchedule& s);   // recaptures the graph
+
+    // Every product of the batch on its device buffers: one graph launch on st.
+    void run_device(cudaStream_t st);
+    // The same from host arrays (a[i], b[i] in, c[i] out); returns when every
+    // c[i] is written.
+    void run_host(const uint32_t* const* a, const uint32_t* const* b, uint32_t* const* c);
+
+    // Times each candidate schedule (one warm-up and `reps` timed graph
+    // replays, minimum kept) and keeps the fastest; returns its time in us.
+    double tune(int reps);
+
+    // Launches in one replay of the graph (kernel nodes).
+    int launches() const { return launches_; }
+
+    // Reads and clears the batch's error word (nonzero: a pipeline wait in a
+    // tensor-core kernel timed out); synchronous.
+    uint32_t take_error();
+
+private:
+    struct Prod {
+        Engine* e;
+        DevPoint d;          // the engine's point, error word redirected to the batch's
+        uint32_t *a, *b, *c, *A, *B;
+        double cost;         // relative work, for ordering
+    };
+    void enqueue(cudaStream_t st);
+    void build_graph();
+    void release_graph();
+    cudaStream_t branch(size_t i);
+    static uint64_t occupancy_key(int pass, uint32_t logR, uint32_t logS, bool lazy);
+
+    std::vector<Prod> prods_;
+    BatchSchedule sched_{};
+    void* slab_ = nullptr;
+    size_t slab_bytes_ = 0;
+    uint32_t* err_ = nullptr;
+    int sms_ = 0;
+    int launches_ = 0;
+    cudaStream_t stream_ = nullptr;   // capture origin and host-path copies
+    std::vector<cudaStream_t> branches_;
+    std::vector<cudaEvent_t> events_;
+    std::map<uint64_t, int> occupancy_;   // resident blocks per SM, per grouped transform kernel
+    cudaGraphExec_t exec_ = nullptr;
+};
+
+}  // namespace fpm

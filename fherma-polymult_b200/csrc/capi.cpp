@@ -3,6 +3,7 @@
 #include "fherma_abi.h"
 #include "fherma_polymult.h"
 
+#include "batch.h"
 #include "engine.h"
 #include "kernels.h"
 
@@ -14,10 +15,16 @@
 #include <stdexcept>
 #include <string>
 #include <thread>
+#include <vector>
 
 struct fpm_ctx {
     fpm::Engine* engine;
     uint32_t W;
+};
+
+struct fpm_batch {
+    fpm::Batch* batch;
+    double tuned_us;
 };
 
 namespace {
@@ -164,6 +171,76 @@ int fpm_stage_transform(fpm_ctx* ctx, uint32_t* d_A, uint32_t* d_B, int mode, vo
 int fpm_stage_crt(fpm_ctx* ctx, const uint32_t* d_y, uint32_t* d_c, void* stream) {
     if (!ctx || !d_y || !d_c) return fail(FPM_EINVAL, "fpm_stage_crt: bad argument");
     return guarded([&] { ctx->engine->crt(d_y, d_c, as_stream(stream)); });
+}
+
+int fpm_batch_create(fpm_ctx* const* ctxs, uint32_t count, fpm_batch** out) {
+    if (!ctxs || !out || count == 0) return fail(FPM_EINVAL, "fpm_batch_create: bad argument");
+    *out = nullptr;
+    fpm::Batch* b = nullptr;
+    const int rc = guarded([&] {
+        std::vector<fpm::Engine*> engines;
+        for (uint32_t i = 0; i < count; ++i) {
+            if (!ctxs[i]) throw std::runtime_error("fpm_batch_create: NULL context");
+            engines.push_back(ctxs[i]->engine);
+        }
+        b = new fpm::Batch(engines);
+    });
+    if (rc) return rc;
+    *out = new fpm_batch{b, 0.0};
+    return FPM_OK;
+}
+
+int fpm_batch_buffers(fpm_batch* batch, uint32_t i, uint32_t** d_a, uint32_t** d_b, uint32_t** d_c) {
+    if (!batch || i >= batch->batch->size()) return fail(FPM_EINVAL, "fpm_batch_buffers: bad argument");
+    if (d_a) *d_a = batch->batch->a(i);
+    if (d_b) *d_b = batch->batch->b(i);
+    if (d_c) *d_c = batch->batch->c(i);
+    return FPM_OK;
+}
+
+int fpm_batch_run_device(fpm_batch* batch, void* stream) {
+    if (!batch) return fail(FPM_EINVAL, "fpm_batch_run_device: NULL argument");
+    return guarded([&] { batch->batch->run_device(as_stream(stream)); });
+}
+
+int fpm_batch_run(fpm_batch* batch, const uint32_t* const* a, const uint32_t* const* b, uint32_t* const* c) {
+    if (!batch || !a || !b || !c) return fail(FPM_EINVAL, "fpm_batch_run: NULL argument");
+    for (size_t i = 0; i < batch->batch->size(); ++i) {
+        if (!a[i] || !b[i] || !c[i]) return fail(FPM_EINVAL, "fpm_batch_run: NULL buffer");
+    }
+    return guarded([&] { batch->batch->run_host(a, b, c); });
+}
+
+int fpm_batch_get_info(const fpm_batch* batch, fpm_batch_info* out) {
+    if (!batch || !out) return fail(FPM_EINVAL, "fpm_batch_get_info: NULL argument");
+    const fpm::BatchSchedule& s = batch->batch->schedule();
+    out->count = static_cast<uint32_t>(batch->batch->size());
+    out->layout = s.layout;
+    out->order = s.order;
+    out->prime_group = s.prime_group;
+    out->grid = s.grid;
+    out->launches = batch->batch->launches();
+    out->device_bytes = batch->batch->device_bytes();
+    out->tuned_us = batch->tuned_us;
+    return FPM_OK;
+}
+
+int fpm_batch_tune(fpm_batch* batch, int reps, fpm_batch_info* info) {
+    if (!batch) return fail(FPM_EINVAL, "fpm_batch_tune: NULL argument");
+    const int rc = guarded([&] { batch->tuned_us = batch->batch->tune(reps); });
+    if (rc) return rc;
+    return info ? fpm_batch_get_info(batch, info) : FPM_OK;
+}
+
+int fpm_batch_set_schedule(fpm_batch* batch, int layout, int order, int prime_group, int grid) {
+    if (!batch) return fail(FPM_EINVAL, "fpm_batch_set_schedule: NULL argument");
+    return guarded([&] { batch->batch->set_schedule(fpm::BatchSchedule{layout, order, prime_group, grid}); });
+}
+
+void fpm_batch_free(fpm_batch* batch) {
+    if (!batch) return;
+    delete batch->batch;
+    delete batch;
 }
 
 }  // extern "C"

@@ -24,6 +24,7 @@
 //                 chunk (32 primes), then the epilogue: carries over D, Xtop,
 //                 negvP_v, reduction mod q, coalesced store of the limbs.
 #include "device.cuh"
+#include "group.cuh"
 #include "kernels.h"
 #include "tc.cuh"
 
@@ -75,15 +76,14 @@ __device__ inline Smem carve(uint8_t* base, uint32_t u) {
 
 constexpr int kX = kMaxL + 2;   // register limbs of the epilogue (predicated to L + 2)
 
-__global__ void __launch_bounds__(kThreads, 1)
-    k_crt_tc(DevPoint d, const uint32_t* __restrict__ Y, uint32_t* __restrict__ C, uint32_t n_begin, uint32_t n_end) {
+// Coefficients n0 .. n0 + nk - 1 (nk <= 128).
+__device__ __forceinline__ void crt_body(const DevPoint& d, const uint32_t* __restrict__ Y, uint32_t* __restrict__ C,
+                                         uint32_t n0, uint32_t nk) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const uint32_t U = d.crt_u;            // GEMM columns (byte positions), multiple of 32, <= 256
     const int nch = (d.K + kChunk - 1) / kChunk;
     const Smem sm = carve(smem_raw, U);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t n0 = n_begin + blockIdx.x * kRows;
-    const uint32_t nk = min(kRows, n_end - n0);
     const int L = d.L, K = d.K;
     const uint32_t tcols = d.crt_tmem_cols;
 
@@ -292,6 +292,20 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
+__global__ void __launch_bounds__(kThreads, 1)
+    k_crt_tc(DevPoint d, const uint32_t* __restrict__ Y, uint32_t* __restrict__ C, uint32_t n_begin, uint32_t n_end) {
+    const uint32_t n0 = n_begin + blockIdx.x * kRows;
+    crt_body(d, Y, C, n0, min(kRows, n_end - n0));
+}
+
+// Grouped: item i owns ceil(N / 128) blocks; y_j in its A, c out.
+__global__ void __launch_bounds__(kThreads, 1) k_crt_tc_group(const __grid_constant__ GroupTable t) {
+    const uint32_t i = group_locate(t, blockIdx.x);
+    const GroupItem& it = t.item[i];
+    const uint32_t n0 = (blockIdx.x - t.first[i]) * kRows;
+    crt_body(it.d, it.A, it.c, n0, min(kRows, it.d.N - n0));
+}
+
 // Large enough that the blocks sharing an SM never ask for more than its 512
 // TMEM columns in total.
 size_t smem_bytes(uint32_t u, uint32_t tmem_cols) {
@@ -304,9 +318,21 @@ size_t smem_bytes(uint32_t u, uint32_t tmem_cols) {
 }  // namespace
 
 void crt_tc_init_attributes() {
-    check(cudaFuncSetAttribute(k_crt_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem_bytes(256, 256))),
-          "crt_tc smem");
+    const int bytes = static_cast<int>(smem_bytes(256, 256));
+    check(cudaFuncSetAttribute(k_crt_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "crt_tc smem");
+    check(cudaFuncSetAttribute(k_crt_tc_group, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "crt_tc smem");
+}
+
+uint32_t crt_tc_group_blocks(uint32_t N) { return (N + kRows - 1) / kRows; }
+
+void launch_crt_tc_group(const GroupTable& t, cudaStream_t st) {
+    if (t.total == 0) return;
+    uint32_t u = 0, cols = 0;
+    for (uint32_t i = 0; i < t.count; ++i) {
+        u = t.item[i].d.crt_u > u ? t.item[i].d.crt_u : u;
+        cols = t.item[i].d.crt_tmem_cols > cols ? t.item[i].d.crt_tmem_cols : cols;
+    }
+    k_crt_tc_group<<<t.total, kThreads, smem_bytes(u, cols), st>>>(t);
 }
 
 void launch_crt_tc(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_begin, uint32_t n_end,

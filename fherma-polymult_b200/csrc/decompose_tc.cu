@@ -23,6 +23,7 @@
 //                 a chunk's 32 primes), one thread per lane (= coefficient):
 //                 tcgen05.ld, fold, coalesced stores of each prime's residues.
 #include "device.cuh"
+#include "group.cuh"
 #include "kernels.h"
 #include "tc.cuh"
 
@@ -69,17 +70,15 @@ __device__ __forceinline__ uint32_t fold49(uint64_t v, uint4 f) {
     return add_mod(lo, hi, f.x);
 }
 
-__global__ void __launch_bounds__(kThreads)
-    k_decompose_tc(DevPoint d, const uint32_t* __restrict__ limbs, uint32_t* __restrict__ res, int operand,
-                   uint32_t n_begin, uint32_t n_end) {
+// Coefficients n0 .. n0 + nk - 1 (nk <= 128) of one operand.
+__device__ __forceinline__ void dec_body(const DevPoint& d, const uint32_t* __restrict__ limbs,
+                                         uint32_t* __restrict__ res, int operand, uint32_t n0, uint32_t nk) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const uint32_t kb = d.dec_kb;          // GEMM K in bytes (4L rounded up to 32)
     const int nch = d.dec_chunks;
     const Smem sm = carve(smem_raw, kb);
     const uint8_t* img = operand ? d.dec_img_b : d.dec_img_a;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t n0 = n_begin + blockIdx.x * kRows;
-    const uint32_t nk = min(kRows, n_end - n0);
     const int L = d.L;
 
     if (threadIdx.x == 0) {
@@ -237,6 +236,23 @@ __global__ void __launch_bounds__(kThreads)
     }
 }
 
+__global__ void __launch_bounds__(kThreads)
+    k_decompose_tc(DevPoint d, const uint32_t* __restrict__ limbs, uint32_t* __restrict__ res, int operand,
+                   uint32_t n_begin, uint32_t n_end) {
+    const uint32_t n0 = n_begin + blockIdx.x * kRows;
+    dec_body(d, limbs, res, operand, n0, min(kRows, n_end - n0));
+}
+
+// Grouped: item i owns 2 ceil(N / 128) blocks, operand a's tiles then b's.
+__global__ void __launch_bounds__(kThreads) k_decompose_tc_group(const __grid_constant__ GroupTable t) {
+    const uint32_t i = group_locate(t, blockIdx.x);
+    const GroupItem& it = t.item[i];
+    const uint32_t local = blockIdx.x - t.first[i], tiles = (it.d.N + kRows - 1) / kRows;
+    const int operand = local >= tiles;
+    const uint32_t n0 = (local - (operand ? tiles : 0)) * kRows;
+    dec_body(it.d, operand ? it.b : it.a, operand ? it.B : it.A, operand, n0, min(kRows, it.d.N - n0));
+}
+
 // At least 78 KB, so no more than two blocks (2 x 256 TMEM columns) share an SM.
 size_t smem_bytes(uint32_t kb) {
     const size_t need = ((a_bytes(kb) + 127) & ~127u) + 2 * kCols * kb + 8 * sizeof(uint64_t) + kMaxK * sizeof(uint4);
@@ -246,9 +262,20 @@ size_t smem_bytes(uint32_t kb) {
 }  // namespace
 
 void decompose_tc_init_attributes() {
-    check(cudaFuncSetAttribute(k_decompose_tc, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(smem_bytes(4 * kMaxL))),
+    const int bytes = static_cast<int>(smem_bytes(4 * kMaxL));
+    check(cudaFuncSetAttribute(k_decompose_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
           "decompose_tc smem");
+    check(cudaFuncSetAttribute(k_decompose_tc_group, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+          "decompose_tc smem");
+}
+
+uint32_t decompose_tc_group_blocks(uint32_t N) { return 2 * ((N + kRows - 1) / kRows); }
+
+void launch_decompose_tc_group(const GroupTable& t, cudaStream_t st) {
+    if (t.total == 0) return;
+    uint32_t kb = 0;
+    for (uint32_t i = 0; i < t.count; ++i) kb = t.item[i].d.dec_kb > kb ? t.item[i].d.dec_kb : kb;
+    k_decompose_tc_group<<<t.total, kThreads, smem_bytes(kb), st>>>(t);
 }
 
 void launch_decompose_tc(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, uint32_t n_begin,

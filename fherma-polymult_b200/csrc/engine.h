@@ -25,6 +25,7 @@ public:
     const HostPlan& plan() const { return plan_; }
     const DevPoint& point() const { return dp_; }
     int device() const { return device_; }
+    bool simt() const { return simt_; }
 
     // c = a b on device buffers (N x L each), enqueued on st; the engine's
     // residue workspaces are used, so calls on one engine must not overlap.

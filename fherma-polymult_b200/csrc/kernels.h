@@ -57,4 +57,18 @@ void launch_crt(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_be
 void launch_crt_tc(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_begin, uint32_t n_end,
                    cudaStream_t st);
 
+// Grouped launches (group.cuh): one launch covers every item of the table,
+// whose first[] the caller fills with these per-item block counts.
+struct GroupTable;
+uint32_t decompose_tc_group_blocks(uint32_t N);   // both operands
+uint32_t crt_tc_group_blocks(uint32_t N);
+uint32_t ntt_blocks_per_prime(int pass, uint32_t logR, uint32_t logS);
+void launch_decompose_tc_group(const GroupTable& t, cudaStream_t st);
+void launch_crt_tc_group(const GroupTable& t, cudaStream_t st);
+// pass kPassColFwd / kPassRow (product) / kPassColInv over items of one
+// (logR, logS); grid 0 = one block per tile, else a persistent grid.
+void launch_ntt_group(const GroupTable& t, int pass, uint32_t logR, uint32_t logS, bool lazy, uint32_t grid,
+                      cudaStream_t st);
+int ntt_group_occupancy(int pass, uint32_t logR, uint32_t logS, bool lazy);
+
 }  // namespace fpm

@@ -18,8 +18,11 @@
 //   * with primes below 2^30 the butterflies are Harvey's lazy ones (values
 //     below 4p forward, 2p inverse).
 #include "device.cuh"
+#include "group.cuh"
 #include "kernels.h"
 #include "ntt_engine.cuh"
+
+#include <type_traits>
 
 namespace fpm {
 
@@ -105,7 +108,7 @@ __device__ __forceinline__ void col_global_store(uint32_t* const (&X)[NV], const
 }
 
 template <int LOGR, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads) k_ntt_col_fwd(DevPoint d, uint32_t* A, uint32_t* B) {
+__device__ __forceinline__ void col_fwd_body(const DevPoint& d, uint32_t* A, uint32_t* B, int j, uint32_t bx) {
     extern __shared__ __align__(1024) uint32_t smem[];
     constexpr int XS = 11 - LOGR;
     constexpr uint32_t R = 1u << LOGR, C = 1u << XS;
@@ -113,8 +116,7 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_col_fwd(DevPoint d, uint32_
     uint32_t* ta = smem;
     uint32_t* tb = smem + 2048;
     uint2* tw = reinterpret_cast<uint2*>(smem + 4096);
-    const int j = blockIdx.y;
-    const uint32_t S = 1u << d.logS, c0 = blockIdx.x * C;
+    const uint32_t S = 1u << d.logS, c0 = bx * C;
     const uint32_t p = d.pc[j].p;
     uint32_t* const X[2] = {A + static_cast<size_t>(j) * d.N, B + static_cast<size_t>(j) * d.N};
     for (uint32_t y = threadIdx.x; y < R; y += kNttThreads) tw[y] = d.col_f[static_cast<size_t>(j) * R + y];
@@ -143,15 +145,14 @@ __global__ void __launch_bounds__(kNttThreads) k_ntt_col_fwd(DevPoint d, uint32_
 }
 
 template <int LOGR, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads) k_ntt_col_inv(DevPoint d, uint32_t* A) {
+__device__ __forceinline__ void col_inv_body(const DevPoint& d, uint32_t* A, int j, uint32_t bx) {
     extern __shared__ __align__(1024) uint32_t smem[];
     constexpr int XS = 11 - LOGR;
     constexpr uint32_t R = 1u << LOGR, C = 1u << XS;
     constexpr int last = RP<LOGR, XS, SwzCol>::kCount - 1;
     uint32_t* ta = smem;
     uint2* tw = reinterpret_cast<uint2*>(smem + 2048);
-    const int j = blockIdx.y;
-    const uint32_t S = 1u << d.logS, c0 = blockIdx.x * C;
+    const uint32_t S = 1u << d.logS, c0 = bx * C;
     const uint32_t p = d.pc[j].p;
     uint32_t* const X[1] = {A + static_cast<size_t>(j) * d.N};
     for (uint32_t y = threadIdx.x; y < R; y += kNttThreads) tw[y] = d.col_i[static_cast<size_t>(j) * R + y];
@@ -241,7 +242,7 @@ __device__ __forceinline__ size_t row_offset(uint32_t i, uint32_t u0, uint32_t R
 }
 
 template <int LOGS, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads, 5) k_ntt_row(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
+__device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, int j, uint32_t bx) {
     extern __shared__ __align__(1024) uint32_t smem[];
     using RG = RowGeom<LOGS>;
     using RPR = RP<LOGS, 0, SwzRow>;
@@ -249,8 +250,7 @@ __global__ void __launch_bounds__(kNttThreads, 5) k_ntt_row(DevPoint d, uint32_t
     uint32_t* ta = smem;
     uint32_t* tb = smem + 2048;
     uint2* tf = reinterpret_cast<uint2*>(smem + 4096);
-    const int j = blockIdx.y;
-    const uint32_t u0 = blockIdx.x * RG::kPairsPerBlock;
+    const uint32_t u0 = bx * RG::kPairsPerBlock;
     const uint32_t R = 1u << d.logR;
     const PrimeConsts pc = d.pc[j];
     const uint32_t p = pc.p;
@@ -338,6 +338,71 @@ __global__ void __launch_bounds__(kNttThreads, 5) k_ntt_row(DevPoint d, uint32_t
     }
 }
 
+// Blocks per prime of each pass.
+template <int LOGR>
+__host__ __device__ __forceinline__ uint32_t col_blocks(uint32_t logS) {
+    return (1u << logS) >> (11 - LOGR);
+}
+
+template <int LOGS>
+__host__ __device__ __forceinline__ uint32_t row_blocks(uint32_t logR) {
+    using RG = RowGeom<LOGS>;
+    return RG::G >= 2 ? (1u << logR) / RG::G : (1u << logR);
+}
+
+// Plain launches: grid (blocks per prime, K).
+template <int LOGR, bool LAZY>
+__global__ void __launch_bounds__(kNttThreads) k_ntt_col_fwd(DevPoint d, uint32_t* A, uint32_t* B) {
+    col_fwd_body<LOGR, LAZY>(d, A, B, blockIdx.y, blockIdx.x);
+}
+
+template <int LOGR, bool LAZY>
+__global__ void __launch_bounds__(kNttThreads) k_ntt_col_inv(DevPoint d, uint32_t* A) {
+    col_inv_body<LOGR, LAZY>(d, A, blockIdx.y, blockIdx.x);
+}
+
+template <int LOGS, bool LAZY>
+__global__ void __launch_bounds__(kNttThreads, 5) k_ntt_row(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
+    row_body<LOGS, LAZY>(d, A, B, mode, blockIdx.y, blockIdx.x);
+}
+
+// Grouped launches over products of one geometry class: a (possibly
+// persistent) 1-D grid walks the table's blocks; block b of item i is prime
+// j0 + local / per, tile local % per (an item is a group of one product's
+// primes).
+template <int LOGR, bool LAZY>
+__global__ void __launch_bounds__(kNttThreads, 6) k_ntt_col_fwd_group(const __grid_constant__ GroupTable t) {
+    for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
+        if (b != blockIdx.x) __syncthreads();   // the previous tile's shared memory
+        const uint32_t i = group_locate(t, b);
+        const GroupItem& it = t.item[i];
+        const uint32_t local = b - t.first[i], per = col_blocks<LOGR>(it.d.logS);
+        col_fwd_body<LOGR, LAZY>(it.d, it.A, it.B, it.j0 + local / per, local % per);
+    }
+}
+
+template <int LOGR, bool LAZY>
+__global__ void __launch_bounds__(kNttThreads, 6) k_ntt_col_inv_group(const __grid_constant__ GroupTable t) {
+    for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
+        if (b != blockIdx.x) __syncthreads();
+        const uint32_t i = group_locate(t, b);
+        const GroupItem& it = t.item[i];
+        const uint32_t local = b - t.first[i], per = col_blocks<LOGR>(it.d.logS);
+        col_inv_body<LOGR, LAZY>(it.d, it.A, it.j0 + local / per, local % per);
+    }
+}
+
+template <int LOGS, bool LAZY>
+__global__ void __launch_bounds__(kNttThreads, 5) k_ntt_row_group(const __grid_constant__ GroupTable t) {
+    for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
+        if (b != blockIdx.x) __syncthreads();
+        const uint32_t i = group_locate(t, b);
+        const GroupItem& it = t.item[i];
+        const uint32_t local = b - t.first[i], per = row_blocks<LOGS>(it.d.logR);
+        row_body<LOGS, LAZY>(it.d, it.A, it.B, kRowProduct, it.j0 + local / per, local % per);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // N <= 1024: one block per prime holds both operands; one butterfly per
 // thread per stage, full twiddle tables from global memory, full reduction.
@@ -396,19 +461,61 @@ constexpr size_t row_smem_t() {
 
 template <int LOGR, bool LAZY>
 void col_attrs() {
-    check(cudaFuncSetAttribute(k_ntt_col_fwd<LOGR, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(col_fwd_smem_t(LOGR))),
+    const int fwd = static_cast<int>(col_fwd_smem_t(LOGR)), inv = static_cast<int>(col_inv_smem_t(LOGR));
+    check(cudaFuncSetAttribute(k_ntt_col_fwd<LOGR, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, fwd),
           "col smem");
-    check(cudaFuncSetAttribute(k_ntt_col_inv<LOGR, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(col_inv_smem_t(LOGR))),
+    check(cudaFuncSetAttribute(k_ntt_col_inv<LOGR, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, inv),
+          "col smem");
+    check(cudaFuncSetAttribute(k_ntt_col_fwd_group<LOGR, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, fwd),
+          "col smem");
+    check(cudaFuncSetAttribute(k_ntt_col_inv_group<LOGR, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, inv),
           "col smem");
 }
 
 template <int LOGS, bool LAZY>
 void row_attrs() {
-    check(cudaFuncSetAttribute(k_ntt_row<LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(row_smem_t<LOGS>())),
+    const int bytes = static_cast<int>(row_smem_t<LOGS>());
+    check(cudaFuncSetAttribute(k_ntt_row<LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
           "row smem");
+    check(cudaFuncSetAttribute(k_ntt_row_group<LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
+          "row smem");
+}
+
+// Calls f(std::integral_constant<int, V>) for V = v in [6, 11].
+template <class F>
+void with_log(uint32_t v, F&& f) {
+    switch (v) {
+        case 6: f(std::integral_constant<int, 6>{}); break;
+        case 7: f(std::integral_constant<int, 7>{}); break;
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        case 9: f(std::integral_constant<int, 9>{}); break;
+        case 10: f(std::integral_constant<int, 10>{}); break;
+        case 11: f(std::integral_constant<int, 11>{}); break;
+        default: throw std::runtime_error("unsupported transform geometry");
+    }
+}
+
+// One grouped pass: the kernel, its shared memory, and (occupancy) its
+// resident blocks per SM.
+template <bool LAZY>
+void group_pass(const GroupTable* t, int pass, uint32_t logR, uint32_t logS, uint32_t grid, cudaStream_t st,
+                int* occupancy) {
+    auto run = [&](auto kernel, size_t smem) {
+        if (occupancy) {
+            check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kernel, kNttThreads, smem), "occupancy");
+        } else {
+            kernel<<<grid, kNttThreads, smem, st>>>(*t);
+        }
+    };
+    if (pass == kPassColFwd) {
+        with_log(logR, [&](auto c) { run(k_ntt_col_fwd_group<decltype(c)::value, LAZY>, col_fwd_smem_t(c)); });
+    } else if (pass == kPassColInv) {
+        with_log(logR, [&](auto c) { run(k_ntt_col_inv_group<decltype(c)::value, LAZY>, col_inv_smem_t(c)); });
+    } else if (pass == kPassRow) {
+        with_log(logS, [&](auto c) { run(k_ntt_row_group<decltype(c)::value, LAZY>, row_smem_t<decltype(c)::value>()); });
+    } else {
+        throw std::runtime_error("grouped transform: unknown pass");
+    }
 }
 
 template <bool LAZY>
@@ -509,6 +616,35 @@ void launch_ntt(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStrea
     } else {
         launch_ntt_t<false>(d, A, B, mode, st);
     }
+}
+
+uint32_t ntt_blocks_per_prime(int pass, uint32_t logR, uint32_t logS) {
+    if (pass == kPassRow) {
+        const uint32_t G = 2048u >> logS;
+        return G >= 2 ? (1u << logR) / G : (1u << logR);
+    }
+    return (1u << logS) >> (11 - logR);
+}
+
+void launch_ntt_group(const GroupTable& t, int pass, uint32_t logR, uint32_t logS, bool lazy, uint32_t grid,
+                      cudaStream_t st) {
+    if (t.total == 0) return;
+    if (grid == 0 || grid > t.total) grid = t.total;
+    if (lazy) {
+        group_pass<true>(&t, pass, logR, logS, grid, st, nullptr);
+    } else {
+        group_pass<false>(&t, pass, logR, logS, grid, st, nullptr);
+    }
+}
+
+int ntt_group_occupancy(int pass, uint32_t logR, uint32_t logS, bool lazy) {
+    int n = 0;
+    if (lazy) {
+        group_pass<true>(nullptr, pass, logR, logS, 0, nullptr, &n);
+    } else {
+        group_pass<false>(nullptr, pass, logR, logS, 0, nullptr, &n);
+    }
+    return n;
 }
 
 }  // namespace fpm

@@ -41,6 +41,12 @@ class FpmInfo(ctypes.Structure):
                 ("device", ctypes.c_int32), ("device_bytes", ctypes.c_uint64), ("prime_bits", ctypes.c_uint32)]
 
 
+class FpmBatchInfo(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_uint32), ("layout", ctypes.c_int32), ("order", ctypes.c_int32),
+                ("prime_group", ctypes.c_int32), ("grid", ctypes.c_int32), ("launches", ctypes.c_int32),
+                ("device_bytes", ctypes.c_uint64), ("tuned_us", ctypes.c_double)]
+
+
 class FpmError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(message)
@@ -77,6 +83,15 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "fpm_stage_decompose": ([vp, vp, vp, ctypes.c_int, vp], ctypes.c_int),
         "fpm_stage_transform": ([vp, vp, vp, ctypes.c_int, vp], ctypes.c_int),
         "fpm_stage_crt": ([vp, vp, vp, vp], ctypes.c_int),
+        "fpm_batch_create": ([ctypes.POINTER(vp), ctypes.c_uint32, ctypes.POINTER(vp)], ctypes.c_int),
+        "fpm_batch_buffers": ([vp, ctypes.c_uint32, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)],
+                              ctypes.c_int),
+        "fpm_batch_run_device": ([vp, vp], ctypes.c_int),
+        "fpm_batch_run": ([vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)], ctypes.c_int),
+        "fpm_batch_tune": ([vp, ctypes.c_int, ctypes.POINTER(FpmBatchInfo)], ctypes.c_int),
+        "fpm_batch_set_schedule": ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "fpm_batch_get_info": ([vp, ctypes.POINTER(FpmBatchInfo)], ctypes.c_int),
+        "fpm_batch_free": ([vp], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -172,6 +187,76 @@ class Context:
 
     def stage_crt(self, d_y: int, d_c: int, stream: int = 0):
         _check(self._lib.fpm_stage_crt(self._h, d_y, d_c, stream or None))
+
+
+class Batch:
+    """Many products of uneven (N, q) in one CUDA graph of grouped launches
+    (fpm_batch).  ``contexts`` are Context objects (one per product, repeats
+    allowed); they must stay open while the batch lives."""
+
+    def __init__(self, contexts):
+        lib = load()
+        self._lib = lib
+        self.contexts = list(contexts)
+        arr = (ctypes.c_void_p * len(self.contexts))(*[c.handle.value for c in self.contexts])
+        h = ctypes.c_void_p()
+        _check(lib.fpm_batch_create(arr, len(self.contexts), ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.fpm_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return len(self.contexts)
+
+    @property
+    def info(self) -> FpmBatchInfo:
+        out = FpmBatchInfo()
+        _check(self._lib.fpm_batch_get_info(self._h, ctypes.byref(out)))
+        return out
+
+    def buffers(self, i: int) -> tuple[int, int, int]:
+        """Device pointers (a, b, c) of product i."""
+        a, b, c = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        _check(self._lib.fpm_batch_buffers(self._h, i, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def run_device(self, stream: int = 0):
+        """Every product on the batch's device buffers: one graph launch."""
+        _check(self._lib.fpm_batch_run_device(self._h, stream or None))
+
+    def run(self, a_list, b_list, out=None) -> list:
+        """c_i = a_i b_i for host arrays (N_i x L_i u32 each)."""
+        n = len(self.contexts)
+        if len(a_list) != n or len(b_list) != n:
+            raise FpmError(FPM_EINVAL, f"expected {n} operand pairs")
+        a = [_limbs(x, c.N, c.L, "a") for x, c in zip(a_list, self.contexts)]
+        b = [_limbs(x, c.N, c.L, "b") for x, c in zip(b_list, self.contexts)]
+        cs = out if out is not None else [np.empty((c.N, c.L), np.uint32) for c in self.contexts]
+        pa = (ctypes.c_void_p * n)(*[x.ctypes.data for x in a])
+        pb = (ctypes.c_void_p * n)(*[x.ctypes.data for x in b])
+        pc = (ctypes.c_void_p * n)(*[x.ctypes.data for x in cs])
+        _check(self._lib.fpm_batch_run(self._h, pa, pb, pc))
+        return cs
+
+    def tune(self, reps: int = 3) -> FpmBatchInfo:
+        out = FpmBatchInfo()
+        _check(self._lib.fpm_batch_tune(self._h, reps, ctypes.byref(out)))
+        return out
+
+    def set_schedule(self, layout: int = 1, order: int = 1, prime_group: int = 0, grid: int = 0):
+        _check(self._lib.fpm_batch_set_schedule(self._h, layout, order, prime_group, grid))
 
 
 # ---------------------------------------------------------------------------

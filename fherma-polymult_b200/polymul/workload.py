@@ -137,3 +137,25 @@ def case(N: int, W: int, pattern: str = "uniform", seed: int = 0):
     q = random_modulus(W, rng)
     a, b = operands(q, N, pattern, rng)
     return q, a, b
+
+
+MIX_N = (4096, 8192, 16384, 32768, 65536)
+MIX_W = (128, 512, 868, 1747, 2048)
+
+
+def mix_points(count: int, seed: int):
+    """(N, W, q) for `count` products drawn from the batched / serving mix:
+    N from MIX_N and W from MIX_W, uniformly, each with its own seeded q."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(count):
+        N = int(rng.choice(MIX_N))
+        W = int(rng.choice(MIX_W))
+        out.append((N, W, random_modulus(W, rng)))
+    return out
+
+
+def mix_operands(points, seed: int):
+    """Uniform operands below each point's q."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return [operands(q, N, "uniform", rng) for N, W, q in points]

@@ -124,6 +124,50 @@ FPM_API int fpm_stage_transform(fpm_ctx* ctx, uint32_t* d_A, uint32_t* d_B, int 
  * (forward column pass, fused row pass, inverse column pass), for timing. */
 FPM_API int fpm_stage_crt(fpm_ctx* ctx, const uint32_t* d_y, uint32_t* d_c, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Batches (no reference counterpart; the reference runs one product per
+ * fherma_run call).  A batch runs many products of uneven N and q width in
+ * one CUDA graph of grouped launches: each stage kernel covers the tiles of
+ * every product at once, so small products fill the GPU beside large ones.
+ * Each product's point is a context from fpm_init (its tables stay resident);
+ * the batch owns device buffers for every product's a, b and c and its
+ * residue workspaces.  A context may appear in several batches and more than
+ * once in one; contexts must outlive the batch. */
+typedef struct fpm_batch fpm_batch;
+
+typedef struct fpm_batch_info {
+    uint32_t count;        /* products */
+    int32_t layout;        /* 0 one stream; 1 transform geometries as parallel graph
+                              branches; 2 a whole branch per geometry */
+    int32_t order;         /* 0 as given; 1 largest product first */
+    int32_t prime_group;   /* primes per transform work item (0: all of a product's) */
+    int32_t grid;          /* transform grids: 0 one block per tile, k > 0 persistent */
+    int32_t launches;      /* kernel launches in one graph replay */
+    uint64_t device_bytes; /* device memory the batch holds */
+    double tuned_us;       /* graph time of the chosen schedule (0 until fpm_batch_tune) */
+} fpm_batch_info;
+
+/* Builds a batch over ctxs[0 .. count-1] (all on the current device) and
+ * captures its graph with the default schedule. */
+FPM_API int fpm_batch_create(fpm_ctx* const* ctxs, uint32_t count, fpm_batch** out);
+/* Device buffers of product i (N_i x L_i u32 each): write a and b, read c. */
+FPM_API int fpm_batch_buffers(fpm_batch* batch, uint32_t i, uint32_t** d_a, uint32_t** d_b, uint32_t** d_c);
+/* Every product on the batch's device buffers: one graph launch on `stream`
+ * (a cudaStream_t; returns after enqueueing).  Replays on one batch must be
+ * ordered on one stream. */
+FPM_API int fpm_batch_run_device(fpm_batch* batch, void* stream);
+/* The same from host arrays: a[i], b[i] in, c[i] out (N_i x L_i u32 each);
+ * returns when every c[i] is written. */
+FPM_API int fpm_batch_run(fpm_batch* batch, const uint32_t* const* a, const uint32_t* const* b, uint32_t* const* c);
+/* Autotuner: times every candidate schedule on this batch (one warm-up and
+ * `reps` graph replays each, on the batch's current buffers) and keeps the
+ * fastest; the result is reported in info (may be NULL). */
+FPM_API int fpm_batch_tune(fpm_batch* batch, int reps, fpm_batch_info* info);
+/* Sets a schedule explicitly (fields as in fpm_batch_info) and recaptures. */
+FPM_API int fpm_batch_set_schedule(fpm_batch* batch, int layout, int order, int prime_group, int grid);
+FPM_API int fpm_batch_get_info(const fpm_batch* batch, fpm_batch_info* out);
+FPM_API void fpm_batch_free(fpm_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif
