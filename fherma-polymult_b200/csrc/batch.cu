@@ -50,134 +50,13 @@ struct TransformClass {
 
 }  // namespace
 
-Batch::Batch(const std::vector<Engine*>& engines) {
-    if (engines.empty()) throw std::runtime_error("batch: no products");
-    int dev = -1;
-    check(cudaGetDevice(&dev), "cudaGetDevice");
-    size_t bytes = 0;
-    for (Engine* e : engines) {
-        if (!e) throw std::runtime_error("batch: null context");
-        if (e->device() != dev) throw std::runtime_error("batch: every context must live on the current device");
-        bytes += 3 * align256(e->words() * 4) + 2 * align256(e->residues() * 4);
-    }
-    bytes += 256;   // error word
-    try {
-        check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev), "SM count");
-        check(cudaMalloc(&slab_, bytes), "cudaMalloc (batch)");
-        slab_bytes_ = bytes;
-        check(cudaMemset(slab_, 0, bytes), "memset (batch)");
-        uint8_t* at = static_cast<uint8_t*>(slab_);
-        auto take = [&](size_t n) {
-            uint32_t* p = reinterpret_cast<uint32_t*>(at);
-            at += align256(n * 4);
-            return p;
-        };
-        err_ = take(1);
-        for (Engine* e : engines) {
-            Prod p{};
-            p.e = e;
-            p.d = e->point();
-            p.d.err = err_;
-            p.a = take(e->words());
-            p.b = take(e->words());
-            p.c = take(e->words());
-            p.A = take(e->residues());
-            p.B = take(e->residues());
-            const HostPlan& pl = e->plan();
-            p.cost = static_cast<double>(pl.K) * pl.N * (pl.g.logN + 0.5 * pl.L);
-            prods_.push_back(p);
-        }
-        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
-        build_graph();
-    } catch (...) {
-        release_graph();
-        for (auto s : branches_) cudaStreamDestroy(s);
-        for (auto ev : events_) cudaEventDestroy(ev);
-        if (stream_) cudaStreamDestroy(stream_);
-        if (slab_) cudaFree(slab_);
-        throw;
-    }
-}
-
-Batch::~Batch() {
-    if (stream_) cudaStreamSynchronize(stream_);
-    release_graph();
-    for (auto s : branches_) cudaStreamDestroy(s);
-    for (auto ev : events_) cudaEventDestroy(ev);
-    if (stream_) cudaStreamDestroy(stream_);
-    if (slab_) cudaFree(slab_);
-}
-
-void Batch::release_graph() {
-    if (exec_) cudaGraphExecDestroy(exec_);
-    exec_ = nullptr;
-}
-
-uint64_t Batch::occupancy_key(int pass, uint32_t logR, uint32_t logS, bool lazy) {
+uint64_t occupancy_key(int pass, uint32_t logR, uint32_t logS, bool lazy) {
     return (static_cast<uint64_t>(pass) << 32) | (logR << 16) | (logS << 1) | (lazy ? 1u : 0u);
 }
 
-cudaStream_t Batch::branch(size_t i) {
-    while (branches_.size() <= i) {
-        cudaStream_t s = nullptr;
-        check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
-        branches_.push_back(s);
-    }
-    return branches_[i];
-}
-
-void Batch::set_schedule(const BatchSchedule& s) {
-    if (s.layout < 0 || s.layout > 2 || s.order < 0 || s.order > 1 || s.prime_group < 0 || s.grid < 0)
-        throw std::runtime_error("batch: invalid schedule");
-    sched_ = s;
-    build_graph();
-}
-
-void Batch::build_graph() {
-    check(cudaStreamSynchronize(stream_), "batch sync");
-    release_graph();
-    // Events and branch streams used by the capture, created outside it.
-    const size_t need = 2 * (prods_.size() + 8);
-    while (events_.size() < need) {
-        cudaEvent_t ev = nullptr;
-        check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
-        events_.push_back(ev);
-    }
-    // One branch stream per transform geometry, and the resident blocks per SM
-    // of every grouped transform kernel (persistent grids).
-    size_t classes = 0;
-    std::vector<uint32_t> seen;
-    for (const Prod& p : prods_) {
-        if (p.d.logN <= kSmallLogN) continue;
-        const uint32_t key = p.d.logR * 64 + p.d.logS * 2 + (p.d.lazy ? 1 : 0);
-        if (std::find(seen.begin(), seen.end(), key) != seen.end()) continue;
-        seen.push_back(key);
-        ++classes;
-        for (int pass : {int(kPassColFwd), int(kPassRow), int(kPassColInv)}) {
-            if (pass != kPassRow && p.d.logR == 0) continue;
-            const uint64_t k = occupancy_key(pass, p.d.logR, p.d.logS, p.d.lazy != 0);
-            if (!occupancy_.count(k)) occupancy_[k] = ntt_group_occupancy(pass, p.d.logR, p.d.logS, p.d.lazy != 0);
-        }
-    }
-    for (size_t i = 0; i < classes; ++i) branch(i);
-    cudaGraph_t graph = nullptr;
-    check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
-    try {
-        enqueue(stream_);
-    } catch (...) {
-        cudaStreamEndCapture(stream_, &graph);
-        if (graph) cudaGraphDestroy(graph);
-        cudaGetLastError();
-        throw;
-    }
-    check(cudaStreamEndCapture(stream_, &graph), "end capture");
-    const cudaError_t e = cudaGraphInstantiate(&exec_, graph, 0);
-    cudaGraphDestroy(graph);
-    check(e, "graph instantiate");
-}
-
-void Batch::enqueue(cudaStream_t st) {
-    launches_ = 0;
+int enqueue_grouped(const std::vector<GroupedProduct>& prods_, const BatchSchedule& sched_, cudaStream_t st,
+                    const GroupedLaunchEnv& env) {
+    int launches_ = 0;
     std::vector<size_t> ord(prods_.size());
     std::iota(ord.begin(), ord.end(), size_t(0));
     if (sched_.order == 1) {
@@ -207,7 +86,7 @@ void Batch::enqueue(cudaStream_t st) {
             fill.reset();
         };
         for (size_t i : list) {
-            const Prod& p = prods_[i];
+            const GroupedProduct& p = prods_[i];
             if (p.e->simt()) {
                 launch_decompose(p.d, p.a, p.A, 0, 0, p.d.N, s);
                 launch_decompose(p.d, p.b, p.B, 1, 0, p.d.N, s);
@@ -229,7 +108,7 @@ void Batch::enqueue(cudaStream_t st) {
             fill.reset();
         };
         for (size_t i : list) {
-            const Prod& p = prods_[i];
+            const GroupedProduct& p = prods_[i];
             if (p.e->simt() || !crt_uses_tc(p.e->plan())) {
                 launch_crt(p.d, p.A, p.c, 0, p.d.N, s);
                 ++launches_;
@@ -275,8 +154,8 @@ void Batch::enqueue(cudaStream_t st) {
             const uint32_t per = ntt_blocks_per_prime(pass, g.logR, g.logS);
             uint32_t grid = 0;
             if (sched_.grid > 0) {
-                grid = static_cast<uint32_t>(sched_.grid) * static_cast<uint32_t>(sms_) *
-                       static_cast<uint32_t>(std::max(1, occupancy_.at(occupancy_key(pass, g.logR, g.logS, g.lazy))));
+                grid = static_cast<uint32_t>(sched_.grid) * static_cast<uint32_t>(env.sms) *
+                       static_cast<uint32_t>(std::max(1, env.occupancy->at(occupancy_key(pass, g.logR, g.logS, g.lazy))));
             }
             fill.reset();
             auto flush = [&] {
@@ -288,7 +167,7 @@ void Batch::enqueue(cudaStream_t st) {
             };
             for (const Item& it : items) {
                 if (fill.full()) flush();
-                const Prod& p = prods_[it.p];
+                const GroupedProduct& p = prods_[it.p];
                 fill.add(p.d, p.a, p.b, p.A, p.B, p.c, it.j0, it.nj * per);
             }
             flush();
@@ -297,8 +176,8 @@ void Batch::enqueue(cudaStream_t st) {
 
     size_t ev = 0;
     auto fork = [&](cudaStream_t from, cudaStream_t to) {
-        check(cudaEventRecord(events_.at(ev), from), "event record");
-        check(cudaStreamWaitEvent(to, events_.at(ev), 0), "stream wait");
+        check(cudaEventRecord(env.events.at(ev), from), "event record");
+        check(cudaStreamWaitEvent(to, env.events.at(ev), 0), "stream wait");
         ++ev;
     };
     std::vector<size_t> all(ord);
@@ -312,7 +191,7 @@ void Batch::enqueue(cudaStream_t st) {
         size_t b = 0;
         std::vector<cudaStream_t> used;
         for (auto& kv : classes) {
-            cudaStream_t s = branch(b++);
+            cudaStream_t s = env.branches.at(b++);
             fork(st, s);
             transform(kv.first, kv.second, s);
             used.push_back(s);
@@ -324,7 +203,7 @@ void Batch::enqueue(cudaStream_t st) {
         size_t b = 0;
         std::vector<cudaStream_t> used;
         for (auto& kv : classes) {
-            cudaStream_t s = branch(b++);
+            cudaStream_t s = env.branches.at(b++);
             fork(st, s);
             decompose(kv.second, s);
             transform(kv.first, kv.second, s);
@@ -337,6 +216,139 @@ void Batch::enqueue(cudaStream_t st) {
         for (cudaStream_t s : used) fork(s, st);
     }
     check(cudaGetLastError(), "batch launch");
+    return launches_;
+}
+
+
+Batch::Batch(const std::vector<Engine*>& engines) {
+    if (engines.empty()) throw std::runtime_error("batch: no products");
+    int dev = -1;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    size_t bytes = 0;
+    for (Engine* e : engines) {
+        if (!e) throw std::runtime_error("batch: null context");
+        if (e->device() != dev) throw std::runtime_error("batch: every context must live on the current device");
+        bytes += 3 * align256(e->words() * 4) + 2 * align256(e->residues() * 4);
+    }
+    bytes += 256;   // error word
+    try {
+        check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev), "SM count");
+        check(cudaMalloc(&slab_, bytes), "cudaMalloc (batch)");
+        slab_bytes_ = bytes;
+        check(cudaMemset(slab_, 0, bytes), "memset (batch)");
+        uint8_t* at = static_cast<uint8_t*>(slab_);
+        auto take = [&](size_t n) {
+            uint32_t* p = reinterpret_cast<uint32_t*>(at);
+            at += align256(n * 4);
+            return p;
+        };
+        err_ = take(1);
+        for (Engine* e : engines) {
+            GroupedProduct p{};
+            p.e = e;
+            p.d = e->point();
+            p.d.err = err_;
+            p.a = take(e->words());
+            p.b = take(e->words());
+            p.c = take(e->words());
+            p.A = take(e->residues());
+            p.B = take(e->residues());
+            const HostPlan& pl = e->plan();
+            p.cost = static_cast<double>(pl.K) * pl.N * (pl.g.logN + 0.5 * pl.L);
+            prods_.push_back(p);
+        }
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+        build_graph();
+    } catch (...) {
+        release_graph();
+        for (auto s : branches_) cudaStreamDestroy(s);
+        for (auto ev : events_) cudaEventDestroy(ev);
+        if (stream_) cudaStreamDestroy(stream_);
+        if (slab_) cudaFree(slab_);
+        throw;
+    }
+}
+
+Batch::~Batch() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    release_graph();
+    for (auto s : branches_) cudaStreamDestroy(s);
+    for (auto ev : events_) cudaEventDestroy(ev);
+    if (stream_) cudaStreamDestroy(stream_);
+    if (slab_) cudaFree(slab_);
+}
+
+void Batch::release_graph() {
+    if (exec_) cudaGraphExecDestroy(exec_);
+    exec_ = nullptr;
+}
+
+cudaStream_t Batch::branch(size_t i) {
+    while (branches_.size() <= i) {
+        cudaStream_t s = nullptr;
+        check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream");
+        branches_.push_back(s);
+    }
+    return branches_[i];
+}
+
+void Batch::set_schedule(const BatchSchedule& s) {
+    if (s.layout < 0 || s.layout > 2 || s.order < 0 || s.order > 1 || s.prime_group < 0 || s.grid < 0)
+        throw std::runtime_error("batch: invalid schedule");
+    sched_ = s;
+    build_graph();
+}
+
+void Batch::build_graph() {
+    check(cudaStreamSynchronize(stream_), "batch sync");
+    release_graph();
+    // Events and branch streams used by the capture, created outside it.
+    const size_t need = 2 * (prods_.size() + 8);
+    while (events_.size() < need) {
+        cudaEvent_t ev = nullptr;
+        check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+        events_.push_back(ev);
+    }
+    // One branch stream per transform geometry, and the resident blocks per SM
+    // of every grouped transform kernel (persistent grids).
+    size_t classes = 0;
+    std::vector<uint32_t> seen;
+    for (const GroupedProduct& p : prods_) {
+        if (p.d.logN <= kSmallLogN) continue;
+        const uint32_t key = p.d.logR * 64 + p.d.logS * 2 + (p.d.lazy ? 1 : 0);
+        if (std::find(seen.begin(), seen.end(), key) != seen.end()) continue;
+        seen.push_back(key);
+        ++classes;
+        for (int pass : {int(kPassColFwd), int(kPassRow), int(kPassColInv)}) {
+            if (pass != kPassRow && p.d.logR == 0) continue;
+            const uint64_t k = occupancy_key(pass, p.d.logR, p.d.logS, p.d.lazy != 0);
+            if (!occupancy_.count(k)) occupancy_[k] = ntt_group_occupancy(pass, p.d.logR, p.d.logS, p.d.lazy != 0);
+        }
+    }
+    for (size_t i = 0; i < classes; ++i) branch(i);
+    cudaGraph_t graph = nullptr;
+    check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
+    try {
+        enqueue(stream_);
+    } catch (...) {
+        cudaStreamEndCapture(stream_, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        throw;
+    }
+    check(cudaStreamEndCapture(stream_, &graph), "end capture");
+    const cudaError_t e = cudaGraphInstantiate(&exec_, graph, 0);
+    cudaGraphDestroy(graph);
+    check(e, "graph instantiate");
+}
+
+void Batch::enqueue(cudaStream_t st) {
+    GroupedLaunchEnv env;
+    env.branches = branches_;
+    env.events = events_;
+    env.occupancy = &occupancy_;
+    env.sms = sms_;
+    launches_ = enqueue_grouped(prods_, sched_, st, env);
 }
 
 void Batch::run_device(cudaStream_t st) { check(cudaGraphLaunch(exec_, st), "graph launch"); }

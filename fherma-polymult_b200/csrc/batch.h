@@ -34,6 +34,33 @@ struct BatchSchedule {
                            // k x (resident blocks per SM) x SMs
 };
 
+// One product of a grouped launch sequence: its point (with the error word
+// the launches should report to) and its device buffers.
+struct GroupedProduct {
+    const Engine* e;
+    DevPoint d;
+    uint32_t *a, *b, *c, *A, *B;   // limbs N x L (a, b in; c out), residues K x N
+    double cost;                   // relative work, for ordering
+};
+
+// Streams and events a layout with branches uses (created beforehand, so the
+// sequence can be captured), and the resident blocks per SM of the grouped
+// transform kernels (persistent grids).
+struct GroupedLaunchEnv {
+    std::vector<cudaStream_t> branches;   // one per transform geometry
+    std::vector<cudaEvent_t> events;      // two per geometry
+    const std::map<uint64_t, int>* occupancy = nullptr;
+    int sms = 0;
+};
+
+uint64_t occupancy_key(int pass, uint32_t logR, uint32_t logS, bool lazy);
+
+// Enqueues every product's decompose, transform chain and CRT as grouped
+// launches on st (and, for layouts 1 and 2, the branches); returns the number
+// of kernel launches.
+int enqueue_grouped(const std::vector<GroupedProduct>& prods, const BatchSchedule& s, cudaStream_t st,
+                    const GroupedLaunchEnv& env);
+
 class Batch {
 public:
     // All engines on the current device; the batch does not own them, and
@@ -71,19 +98,12 @@ public:
     uint32_t take_error();
 
 private:
-    struct Prod {
-        Engine* e;
-        DevPoint d;          // the engine's point, error word redirected to the batch's
-        uint32_t *a, *b, *c, *A, *B;
-        double cost;         // relative work, for ordering
-    };
     void enqueue(cudaStream_t st);
     void build_graph();
     void release_graph();
     cudaStream_t branch(size_t i);
-    static uint64_t occupancy_key(int pass, uint32_t logR, uint32_t logS, bool lazy);
 
-    std::vector<Prod> prods_;
+    std::vector<GroupedProduct> prods_;
     BatchSchedule sched_{};
     void* slab_ = nullptr;
     size_t slab_bytes_ = 0;

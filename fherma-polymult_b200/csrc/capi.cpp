@@ -6,6 +6,7 @@
 #include "batch.h"
 #include "engine.h"
 #include "kernels.h"
+#include "server.h"
 
 #include <cuda_runtime.h>
 
@@ -25,6 +26,11 @@ struct fpm_ctx {
 struct fpm_batch {
     fpm::Batch* batch;
     double tuned_us;
+};
+
+struct fpm_server {
+    fpm::Server* server;
+    int lanes;
 };
 
 namespace {
@@ -241,6 +247,73 @@ void fpm_batch_free(fpm_batch* batch) {
     if (!batch) return;
     delete batch->batch;
     delete batch;
+}
+
+int fpm_server_create(fpm_ctx* const* points, uint32_t count, uint64_t budget_bytes, int lanes, int max_batch,
+                      fpm_server** out) {
+    if (!points || !out || count == 0) return fail(FPM_EINVAL, "fpm_server_create: bad argument");
+    *out = nullptr;
+    fpm::Server* srv = nullptr;
+    const int rc = guarded([&] {
+        std::vector<fpm::Engine*> engines;
+        for (uint32_t i = 0; i < count; ++i) {
+            if (!points[i]) throw std::runtime_error("fpm_server_create: NULL context");
+            engines.push_back(points[i]->engine);
+        }
+        fpm::ServerConfig cfg;
+        cfg.budget_bytes = budget_bytes;
+        cfg.lanes = lanes;
+        cfg.max_batch = max_batch;
+        srv = new fpm::Server(engines, cfg);
+    });
+    if (rc) return rc;
+    *out = new fpm_server{srv, lanes};
+    return FPM_OK;
+}
+
+int fpm_server_footprint(const fpm_server* srv, uint32_t point, uint64_t* bytes) {
+    if (!srv || !bytes) return fail(FPM_EINVAL, "fpm_server_footprint: NULL argument");
+    return guarded([&] { *bytes = srv->server->footprint(point); });
+}
+
+int fpm_server_submit(fpm_server* srv, uint32_t point, const uint32_t* a, const uint32_t* b, uint32_t* c,
+                      uint64_t* ticket) {
+    if (!srv || !a || !b || !c || !ticket) return fail(FPM_EINVAL, "fpm_server_submit: NULL argument");
+    return guarded([&] { *ticket = srv->server->submit(point, a, b, c); });
+}
+
+int fpm_server_wait(fpm_server* srv, uint64_t ticket, double* latency_us) {
+    if (!srv) return fail(FPM_EINVAL, "fpm_server_wait: NULL argument");
+    return guarded([&] {
+        const double us = srv->server->wait(ticket);
+        if (latency_us) *latency_us = us;
+    });
+}
+
+int fpm_server_replay(fpm_server* srv, uint32_t n, const uint32_t* point, const double* arrival_us,
+                      const uint32_t* const* a, const uint32_t* const* b, uint32_t* const* c, double* latency_us) {
+    if (!srv || !point || !arrival_us || !a || !b || !c || !latency_us)
+        return fail(FPM_EINVAL, "fpm_server_replay: NULL argument");
+    return guarded([&] { srv->server->replay(n, point, arrival_us, a, b, c, latency_us); });
+}
+
+int fpm_server_get_stats(const fpm_server* srv, fpm_server_stats* out) {
+    if (!srv || !out) return fail(FPM_EINVAL, "fpm_server_get_stats: NULL argument");
+    const fpm::ServerStats s = srv->server->stats();
+    out->completed = s.completed;
+    out->failed = s.failed;
+    out->batches = s.batches;
+    out->lanes = static_cast<uint32_t>(srv->lanes);
+    out->max_lanes_busy = s.max_lanes_busy;
+    out->budget_bytes = srv->server->budget();
+    out->peak_bytes = s.peak_bytes;
+    return FPM_OK;
+}
+
+void fpm_server_free(fpm_server* srv) {
+    if (!srv) return;
+    delete srv->server;
+    delete srv;
 }
 
 }  // extern "C"

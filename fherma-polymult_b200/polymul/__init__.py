@@ -47,6 +47,12 @@ class FpmBatchInfo(ctypes.Structure):
                 ("device_bytes", ctypes.c_uint64), ("tuned_us", ctypes.c_double)]
 
 
+class FpmServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("lanes", ctypes.c_uint32), ("max_lanes_busy", ctypes.c_uint32), ("budget_bytes", ctypes.c_uint64),
+                ("peak_bytes", ctypes.c_uint64)]
+
+
 class FpmError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(message)
@@ -92,6 +98,16 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "fpm_batch_set_schedule": ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "fpm_batch_get_info": ([vp, ctypes.POINTER(FpmBatchInfo)], ctypes.c_int),
         "fpm_batch_free": ([vp], None),
+        "fpm_server_create": ([ctypes.POINTER(vp), ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_int,
+                               ctypes.POINTER(vp)], ctypes.c_int),
+        "fpm_server_footprint": ([vp, ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+        "fpm_server_submit": ([vp, ctypes.c_uint32, vp, vp, vp, ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+        "fpm_server_wait": ([vp, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+        "fpm_server_replay": ([vp, ctypes.c_uint32, _u32p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(vp),
+                               ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_double)],
+                              ctypes.c_int),
+        "fpm_server_get_stats": ([vp, ctypes.POINTER(FpmServerStats)], ctypes.c_int),
+        "fpm_server_free": ([vp], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -257,6 +273,89 @@ class Batch:
 
     def set_schedule(self, layout: int = 1, order: int = 1, prime_group: int = 0, grid: int = 0):
         _check(self._lib.fpm_batch_set_schedule(self._h, layout, order, prime_group, grid))
+
+
+class Server:
+    """Serving loop over resident points (fpm_server): requests are admitted by
+    their device footprint within ``budget_bytes`` and run as micro-batches on
+    ``lanes`` concurrent streams.  Host buffers passed to submit / replay must
+    stay alive until the request is done; pinned buffers overlap best."""
+
+    def __init__(self, contexts, budget_bytes: int = 8 << 30, lanes: int = 4, max_batch: int = 16):
+        lib = load()
+        self._lib = lib
+        self.contexts = list(contexts)
+        arr = (ctypes.c_void_p * len(self.contexts))(*[c.handle.value for c in self.contexts])
+        h = ctypes.c_void_p()
+        _check(lib.fpm_server_create(arr, len(self.contexts), budget_bytes, lanes, max_batch, ctypes.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.fpm_server_free(self._h)
+            self._h = None
+        self._keep = {}
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def footprint(self, point: int) -> int:
+        out = ctypes.c_uint64()
+        _check(self._lib.fpm_server_footprint(self._h, point, ctypes.byref(out)))
+        return out.value
+
+    @property
+    def stats(self) -> FpmServerStats:
+        out = FpmServerStats()
+        _check(self._lib.fpm_server_get_stats(self._h, ctypes.byref(out)))
+        return out
+
+    def _check_buffers(self, point, a, b, c):
+        ctx = self.contexts[point]
+        for name, x in (("a", a), ("b", b), ("c", c)):
+            if x.dtype != np.uint32 or x.size != ctx.N * ctx.L or not x.flags.c_contiguous:
+                raise FpmError(FPM_EINVAL, f"{name}: operand size does not match the point")
+
+    def submit(self, point: int, a: np.ndarray, b: np.ndarray, c: np.ndarray) -> int:
+        """Queues c = a b on `point` (arrays N x L u32, kept alive until wait)."""
+        self._check_buffers(point, a, b, c)
+        t = ctypes.c_uint64()
+        _check(self._lib.fpm_server_submit(self._h, point, a.ctypes.data, b.ctypes.data, c.ctypes.data,
+                                           ctypes.byref(t)))
+        self._keep[t.value] = (a, b, c)
+        return t.value
+
+    def wait(self, ticket: int) -> float:
+        """Latency of the request in microseconds, once c is written."""
+        us = ctypes.c_double()
+        try:
+            _check(self._lib.fpm_server_wait(self._h, ticket, ctypes.byref(us)))
+        finally:
+            self._keep.pop(ticket, None)
+        return us.value
+
+    def replay(self, points, arrival_us, a_list, b_list, c_list) -> np.ndarray:
+        """Submits request i at arrival_us[i]; returns the latencies (us)."""
+        n = len(points)
+        for i in range(n):
+            self._check_buffers(int(points[i]), a_list[i], b_list[i], c_list[i])
+        pts = np.ascontiguousarray(points, dtype=np.uint32)
+        arr = np.ascontiguousarray(arrival_us, dtype=np.float64)
+        lat = np.zeros(n, np.float64)
+        pa = (ctypes.c_void_p * n)(*[x.ctypes.data for x in a_list])
+        pb = (ctypes.c_void_p * n)(*[x.ctypes.data for x in b_list])
+        pc = (ctypes.c_void_p * n)(*[x.ctypes.data for x in c_list])
+        _check(self._lib.fpm_server_replay(self._h, n, pts.ctypes.data_as(_u32p),
+                                           arr.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), pa, pb, pc,
+                                           lat.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return lat
 
 
 # ---------------------------------------------------------------------------

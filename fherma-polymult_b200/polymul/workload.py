@@ -159,3 +159,10 @@ def mix_operands(points, seed: int):
     """Uniform operands below each point's q."""
     rng = np.random.Generator(np.random.PCG64(seed))
     return [operands(q, N, "uniform", rng) for N, W, q in points]
+
+
+def poisson_arrivals(count: int, rate_per_s: float, seed: int) -> np.ndarray:
+    """Arrival times (us) of a seeded Poisson stream: exponential gaps of mean
+    1e6 / rate_per_s, starting at the first gap."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.cumsum(rng.exponential(1e6 / rate_per_s, size=count))

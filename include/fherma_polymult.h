@@ -168,6 +168,46 @@ FPM_API int fpm_batch_set_schedule(fpm_batch* batch, int layout, int order, int 
 FPM_API int fpm_batch_get_info(const fpm_batch* batch, fpm_batch_info* out);
 FPM_API void fpm_batch_free(fpm_batch* batch);
 
+/* ------------------------------------------------------------------------
+ * Serving (no reference counterpart).  A server keeps a set of points
+ * (contexts from fpm_init, tables resident) and a device arena of
+ * budget_bytes.  Each request -- c = a b on one of the points, host buffers --
+ * needs 3 N L + 2 K N words of the arena (fpm_server_footprint) and is
+ * admitted in arrival order once that much is free and one of `lanes` CUDA
+ * streams is idle; a lane takes up to max_batch arrived requests and runs
+ * them as one micro-batch of grouped launches (copies in, decompose,
+ * transforms, CRT, copies out).  Lanes run concurrently, so requests that
+ * arrive while others are on the GPU start as soon as a lane and memory free
+ * up (continuous batching).  Host buffers should be pinned (cudaHostAlloc)
+ * for the copies to overlap.  Contexts must outlive the server. */
+typedef struct fpm_server fpm_server;
+
+typedef struct fpm_server_stats {
+    uint64_t completed, failed;
+    uint64_t batches;          /* micro-batches launched */
+    uint32_t lanes, max_lanes_busy;
+    uint64_t budget_bytes, peak_bytes; /* arena size and its high-water mark */
+} fpm_server_stats;
+
+FPM_API int fpm_server_create(fpm_ctx* const* points, uint32_t count, uint64_t budget_bytes, int lanes,
+                              int max_batch, fpm_server** out);
+/* Device bytes one request on `point` takes from the arena. */
+FPM_API int fpm_server_footprint(const fpm_server* srv, uint32_t point, uint64_t* bytes);
+/* Queues a request (thread-safe; returns at once).  FPM_EINVAL if it can
+ * never fit the budget. */
+FPM_API int fpm_server_submit(fpm_server* srv, uint32_t point, const uint32_t* a, const uint32_t* b, uint32_t* c,
+                              uint64_t* ticket);
+/* Blocks until the request's c is written; latency from submit, in us. */
+FPM_API int fpm_server_wait(fpm_server* srv, uint64_t ticket, double* latency_us);
+/* Replays a trace: request i on point[i] is submitted arrival_us[i]
+ * microseconds after the call starts; returns when all are done, with each
+ * request's latency in latency_us[i]. */
+FPM_API int fpm_server_replay(fpm_server* srv, uint32_t n, const uint32_t* point, const double* arrival_us,
+                              const uint32_t* const* a, const uint32_t* const* b, uint32_t* const* c,
+                              double* latency_us);
+FPM_API int fpm_server_get_stats(const fpm_server* srv, fpm_server_stats* out);
+FPM_API void fpm_server_free(fpm_server* srv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -39,3 +39,21 @@ def test_uniform_hits_the_top_of_the_range():
     vals = np.array(wl.rows_to_ints(a), dtype=object)
     qi = wl.to_int(q)
     assert max(vals) > qi * 0.99 and min(vals) < qi * 0.01
+
+
+def test_poisson_arrivals_seeded_and_rate():
+    t1 = wl.poisson_arrivals(10000, 2000.0, seed=7)
+    t2 = wl.poisson_arrivals(10000, 2000.0, seed=7)
+    assert np.array_equal(t1, t2)
+    gaps = np.diff(np.concatenate([[0.0], t1]))
+    assert (gaps > 0).all()
+    assert abs(gaps.mean() - 500.0) < 15.0          # mean gap 1e6 / rate us
+
+
+def test_mix_points_draw_from_the_mix():
+    pts = wl.mix_points(64, seed=4000)
+    assert len(pts) == 64
+    for N, W, q in pts:
+        assert N in wl.MIX_N and W in wl.MIX_W
+        assert q.shape[0] == (W + 31) // 32 and q[0] & 1
+        assert wl.to_int(q).bit_length() == W
