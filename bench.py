@@ -19,6 +19,10 @@ roofline: the dominant kernel's algorithmic bytes per launch over its CUDA-event
          duration, against the measured HBM copy bandwidth.
 cpu_baseline: the reference's own CPU implementation (solve_cpu.cpp, OpenMP,
          built into oracle/_ref/) on a bounded sample, rank 0 only.
+batched: 64 products of the uneven mix (N 4096 .. 65536, W 128 .. 2048) as one
+         autotuned graph of grouped launches, against 64 sequential plain calls.
+serving: a seeded Poisson stream (10,000 requests at 2000/s) through the
+         serving loop; p50 / p99 latency and products/s.
 """
 from __future__ import annotations
 
@@ -58,6 +62,10 @@ def parse():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="N65536_W2048")
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched (64-product mix) measurement")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving (Poisson stream) measurement")
+    ap.add_argument("--serve-requests", type=int, default=10000)
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
     return ap.parse_args()
 
 
@@ -179,6 +187,168 @@ def run_reference(args):
         "e2e": {"value": us, "unit": "us/product", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
+
+
+def pinned_like(torch, x):
+    """A pinned host copy of x (u32), kept alive by the returned tensor."""
+    t = torch.empty(x.shape, dtype=torch.int32, pin_memory=True)
+    v = t.numpy().view(np.uint32)
+    v[...] = x
+    return t, v
+
+
+def measure_batched(torch, polymul, workload, stream, count=64, reps=20):
+    """Batched mix: `count` products, N from {4096 .. 65536} and W from {128 ..
+    2048} (seeded), one graph of grouped launches after the autotuner, against
+    `count` sequential plain calls on the same GPU (device buffers, and host
+    buffers through fpm_run)."""
+    sp = stream.cuda_stream
+    pts = workload.mix_points(count, seed=4000)
+    ops = workload.mix_operands(pts, seed=4001)
+    ctxs = [polymul.Context(N, W, q) for N, W, q in pts]
+    bt = polymul.Batch(ctxs)
+    keep = []
+    pa, pb, pc = [], [], []
+    for (a, b), c in zip(ops, ctxs):
+        (ta, va), (tb, vb) = pinned_like(torch, a), pinned_like(torch, b)
+        tc, vc = pinned_like(torch, np.zeros_like(a))
+        keep += [ta, tb, tc]
+        pa.append(va)
+        pb.append(vb)
+        pc.append(vc)
+    got = [x.copy() for x in bt.run(pa, pb)]
+    info = bt.tune(reps=3)
+
+    def timed(fn, n):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        fn()
+        stream.synchronize()
+        ev[0].record(stream)
+        for _ in range(n):
+            fn()
+        ev[1].record(stream)
+        ev[1].synchronize()
+        return ev[0].elapsed_time(ev[1]) / n * 1e3   # us per call
+
+    bufs = [bt.buffers(i) for i in range(count)]
+    batch_us = timed(lambda: bt.run_device(sp), reps)
+
+    def seq():
+        for c, (da, db, dc) in zip(ctxs, bufs):
+            c.run_device(da, db, dc, sp)
+
+    seq_us = timed(seq, 5)
+    # End to end: host (pinned) buffers in and out, wall clock.
+    bt.run(pa, pb, pc)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        bt.run(pa, pb, pc)
+    batch_e2e_us = (time.perf_counter() - t0) * 1e6 / 3
+    outs = []
+    for a, _ in ops:
+        to, vo = pinned_like(torch, np.zeros_like(a))
+        keep.append(to)
+        outs.append(vo)
+    for c, a, b, o in zip(ctxs, pa, pb, outs):   # each context's host path set up, untimed
+        c.run(a, b, o)
+    t0 = time.perf_counter()
+    for c, a, b, o in zip(ctxs, pa, pb, outs):
+        c.run(a, b, o)
+    seq_e2e_us = (time.perf_counter() - t0) * 1e6
+    exact = all(np.array_equal(g, o) for g, o in zip(got, outs)) and all(
+        np.array_equal(x, o) for x, o in zip(pc, outs))
+    res = {
+        "products": count, "mix": "N in {4096,8192,16384,32768,65536} x W in {128,512,868,1747,2048}, seed 4000",
+        "batch_us": batch_us, "products_per_s": count / (batch_us * 1e-6),
+        "sequential_us": seq_us, "sequential_products_per_s": count / (seq_us * 1e-6),
+        "speedup_vs_sequential": seq_us / batch_us,
+        "e2e_batch_us": batch_e2e_us, "e2e_sequential_us": seq_e2e_us,
+        "e2e_speedup": seq_e2e_us / batch_e2e_us,
+        "schedule": {"layout": info.layout, "order": info.order, "prime_group": info.prime_group,
+                     "grid": info.grid, "tuned_us": info.tuned_us},
+        "launches_per_batch": info.launches, "device_bytes": info.device_bytes, "bit_exact_vs_plain": bool(exact),
+    }
+    bt.close()
+    for c in ctxs:
+        c.close()
+    return res
+
+
+def measure_serving(torch, polymul, workload, n=10000, rate=2000.0, lanes=4, max_batch=16):
+    """Serving: a seeded Poisson stream of n requests at `rate`/s over 25
+    resident points (the batched mix's N x W grid), pinned host buffers;
+    latency from submit to the result written.  Operands come from two sets per
+    point and results go to a ring of four buffers per point; every ring slot is
+    checked against the product computed alone at the end.  Also the saturated
+    rate (2000 requests at once) against the same requests as sequential plain
+    fpm_run calls."""
+    rng = np.random.Generator(np.random.PCG64(5000))
+    cat = [(N, W) for N in workload.MIX_N for W in workload.MIX_W]
+    ctxs, qs = [], []
+    for N, W in cat:
+        q = workload.random_modulus(W, rng)
+        ctxs.append(polymul.Context(N, W, q))
+        qs.append(q)
+    keep, ops, outs, expect = [], [], [], []
+    SETS, RING = 2, 4
+    for p, (N, W) in enumerate(cat):
+        ps, es, ring = [], [], []
+        for s in range(SETS):
+            a, b = workload.operands(qs[p], N, "uniform", rng)
+            (ta, va), (tb, vb) = pinned_like(torch, a), pinned_like(torch, b)
+            keep += [ta, tb]
+            ps.append((va, vb))
+            es.append(ctxs[p].run(a, b))
+        for _ in range(RING):
+            tc, vc = pinned_like(torch, np.zeros((N, ctxs[p].L), np.uint32))
+            keep.append(tc)
+            ring.append(vc)
+        ops.append(ps)
+        expect.append(es)
+        outs.append(ring)
+    pts = rng.integers(0, len(cat), size=n)
+    arrivals = workload.poisson_arrivals(n, rate, seed=5001)
+    a_l, b_l, c_l, last = [], [], [], {}
+    cnt = np.zeros(len(cat), int)
+    for i, p in enumerate(pts):
+        s = i % SETS
+        slot = cnt[p] % RING
+        cnt[p] += 1
+        a_l.append(ops[p][s][0])
+        b_l.append(ops[p][s][1])
+        c_l.append(outs[p][slot])
+        last[(p, slot)] = s
+    srv = polymul.Server(ctxs, budget_bytes=16 << 30, lanes=lanes, max_batch=max_batch)
+    srv.replay(pts[:50], np.zeros(50), a_l[:50], b_l[:50], c_l[:50])    # warm-up
+    b0 = srv.stats.batches
+    t0 = time.perf_counter()
+    lat = srv.replay(pts, arrivals, a_l, b_l, c_l)
+    wall = time.perf_counter() - t0
+    st = srv.stats
+    verified = sum(np.array_equal(outs[p][slot], expect[p][s]) for (p, slot), s in last.items())
+    m = min(2000, n)
+    t0 = time.perf_counter()
+    srv.replay(pts[:m], np.zeros(m), a_l[:m], b_l[:m], c_l[:m])
+    sat = m / (time.perf_counter() - t0)
+    k = min(500, n)
+    t0 = time.perf_counter()
+    for i in range(k):
+        ctxs[pts[i]].run(a_l[i], b_l[i], c_l[i])
+    plain = k / (time.perf_counter() - t0)
+    res = {
+        "requests": n, "rate_per_s": rate, "lanes": lanes, "max_batch": max_batch, "points": len(cat),
+        "products_per_s": n / wall, "p50_us": float(np.percentile(lat, 50)), "p99_us": float(np.percentile(lat, 99)),
+        "mean_us": float(lat.mean()), "max_us": float(lat.max()),
+        "micro_batches": int(st.batches - b0), "max_lanes_busy": int(st.max_lanes_busy),
+        "peak_device_bytes": int(st.peak_bytes), "budget_bytes": int(st.budget_bytes),
+        "saturated_products_per_s": sat, "plain_sequential_products_per_s": plain,
+        "saturated_vs_plain": sat / plain,
+        "verified": f"{verified}/{len(last)} result buffers bit-exact against the product alone",
+    }
+    srv.close()
+    for c in ctxs:
+        c.close()
+    return res
 
 
 def main():
@@ -337,6 +507,13 @@ def main():
             cpu = {"value": None, "unit": "us/product", "cores": None, "kind": "reference",
                    "sample": f"failed: {e}"}
 
+    batched = serving = None
+    if rank == 0 and world == 1:
+        if not args.no_batched:
+            batched = measure_batched(torch, polymul, workload, stream)
+        if not args.no_serving:
+            serving = measure_serving(torch, polymul, workload, n=args.serve_requests, rate=args.serve_rate)
+
     if rank == 0:
         line = {
             "metric": metric_name(args.workload),
@@ -371,6 +548,8 @@ def main():
             "gpu_launches": args.steps * launches_per_product,
             "clocks": clocks,
             "cpu_baseline": cpu,
+            "batched": batched,
+            "serving": serving,
         }
         print(json.dumps(line))
     ctx.close()
