@@ -385,7 +385,7 @@ def main():
     K = ctx.K
     stream = torch.cuda.Stream()
     sp = stream.cuda_stream
-    launches_per_product = 4 if ctx.info.logN <= 10 else (5 if ctx.info.logR == 0 else 6)
+    launches_per_product = 3 if ctx.info.logN <= 10 or ctx.info.logR == 0 else 5
 
     def step(i):
         da, db, dc = sets_d[i % ROTATE]

@@ -1,0 +1,447 @@
+// CRT on the tensor cores as a persistent, warp-specialised pipeline.
+//
+// Arithmetic (reference CrtView rns.cuh:225-240, crt_columns / crt_combine
+// rns_kernels.cuh:265-364): c = sum_j y_j M_j - v P mod q, v = round(sum_j
+// y_j / p_j).  Here -v P rides in the GEMM as a (K+1)-th row: multiplier v,
+// constant -P mod q, so
+//
+//     X = sum_{j<K} y_j M_j + v (-P mod q) = c (mod q),   X < 2^38 q.
+//
+// The low L - 1 limbs of every constant go through the 8-bit GEMM
+// D[m][u] = sum_{j,s} byte_s(y_j(m)) byte_{u-s}(Mlow_j) (entries < 2^26); the
+// top limb sum_j y_j M_j[L-1] and the rounding sum run on the CUDA cores.  The
+// rounding sum is within 2^-20 of an integer (the prime basis covers 2^20 N q^2),
+// so single precision decides v.
+//
+// Organisation on the B200:
+//   * one CTA per SM walks super-tiles of 256 coefficients; TMEM's 512 columns
+//     hold the two 128-row halves of a super-tile (U <= 256 columns each);
+//   * warp 0 (one thread) streams y in with bulk copies (one 1 KB row per
+//     prime: y_j of the super-tile's 256 coefficients) and the constant image
+//     chunk by chunk, each through a two-slot ring;
+//   * warps 2-9, one thread per row, transpose y into the MMA's K-major byte
+//     layout, add up the rounding sum and the top limb, and put v in the last
+//     chunk;
+//   * warp 1 (one thread) issues the MMAs, two halves per chunk;
+//   * warps 10-17, one thread per row: a quotient estimate e from the top
+//     TMEM columns (within one of floor(X / q)), then one pass from the bottom
+//     limb up that assembles X from D with carries, subtracts e q, stores the
+//     limbs and tracks the borrows that tell whether X - e q lies in [0, q);
+//     the rare row that does not (about 2^-11 of them) adds or subtracts q in
+//     a second pass over what it stored.
+//
+// Every wait is bounded; a timeout raises an abort flag that every role
+// checks, the producer and the MMA thread wait out what they have in flight,
+// and the error word gets bit 1.
+#include "device.cuh"
+#include "kernels.h"
+#include "tc.cuh"
+
+namespace fpm {
+
+namespace {
+
+constexpr int kThreads = 576;             // 18 warps
+constexpr int kStagerWarp0 = 2;           // warps 2-9
+constexpr int kEpiWarp0 = 10;             // warps 10-17
+constexpr uint32_t kSuper = 256;          // coefficients per super-tile
+constexpr uint32_t kChunk = 32;           // K rows (primes) per chunk
+constexpr uint32_t kSlot = 32768;         // bytes: y slot, A slot (two halves), B slot (U <= 256)
+constexpr int kX = kMaxL + 2;
+
+struct Smem {
+    uint8_t* yraw;       // [2][32 primes][256 coefficients] u32
+    uint8_t* a;          // [2][2 halves][16 KB]
+    uint8_t* b;          // [2][U x 128]
+    uint4* meta;         // [2][256] {top limb words 0, 1, 2, -}
+    float* p_recip;      // [kMaxK]
+    uint32_t* m_top;     // [kMaxK]
+    uint32_t* q;         // [kX]: q, zero above L
+    uint64_t* y_full;    // [2]
+    uint64_t* y_empty;   // [2]
+    uint64_t* b_full;    // [2]
+    uint64_t* a_full;    // [2]
+    uint64_t* mma_done;  // [2]
+    uint64_t* d_full;    // [1]
+    uint64_t* d_empty;   // [2]
+    uint64_t* m_full;    // [2]
+    uint64_t* m_empty;   // [2]
+    uint32_t* tmem_base;
+    volatile uint32_t* abort;
+};
+
+constexpr size_t kMetaOff = 6 * size_t(kSlot);
+constexpr size_t kConstOff = kMetaOff + 2 * kSuper * sizeof(uint4);
+constexpr size_t kBarOff = kConstOff + kMaxK * 4 + kMaxK * 4 + kX * 4;
+constexpr size_t kSmemBytes = ((kBarOff + 7) / 8) * 8 + 17 * 8 + 16;
+
+__device__ inline Smem carve(uint8_t* base) {
+    Smem s;
+    s.yraw = base;
+    s.a = base + 2 * kSlot;
+    s.b = base + 4 * kSlot;
+    s.meta = reinterpret_cast<uint4*>(base + kMetaOff);
+    s.p_recip = reinterpret_cast<float*>(base + kConstOff);
+    s.m_top = reinterpret_cast<uint32_t*>(s.p_recip + kMaxK);
+    s.q = s.m_top + kMaxK;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + ((kBarOff + 7) / 8) * 8);
+    s.y_full = bars;
+    s.y_empty = bars + 2;
+    s.b_full = bars + 4;
+    s.a_full = bars + 6;
+    s.mma_done = bars + 8;
+    s.d_full = bars + 10;
+    s.d_empty = bars + 11;
+    s.m_full = bars + 13;
+    s.m_empty = bars + 15;
+    s.tmem_base = reinterpret_cast<uint32_t*>(bars + 17);
+    s.abort = s.tmem_base + 1;
+    return s;
+}
+
+// Bounded wait that also gives up once another role has raised the abort flag.
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile uint32_t* abort) {
+    if (tc::mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = tc::globaltimer();
+    while (!tc::mbar_try_wait(bar, parity)) {
+        if (*abort) return false;
+        if (tc::globaltimer() - t0 > tc::kWaitNs) {
+            *abort = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+// 16 TMEM columns; the wait names the registers so no read moves above it.
+__device__ __forceinline__ void tmem_ld16_sync(uint32_t taddr, uint32_t (&r)[16]) {
+    tc::tmem_ld16(taddr, r);
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15])
+                 :
+                 : "memory");
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_crt_pipe(DevPoint d, const uint32_t* __restrict__ Y, uint32_t* __restrict__ C, uint32_t n_begin,
+               uint32_t n_end) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    const Smem sm = carve(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int L = d.L, K = d.K;
+    const uint32_t U = d.crt_u;
+    const uint32_t N = d.N;
+    const int nch = (K + 1 + static_cast<int>(kChunk) - 1) / static_cast<int>(kChunk);   // K + 1 rows
+    const uint32_t tiles = (n_end - n_begin + kSuper - 1) / kSuper;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 2; ++i) {
+            tc::mbar_init(&sm.y_full[i], 1);
+            tc::mbar_init(&sm.y_empty[i], 256);
+            tc::mbar_init(&sm.b_full[i], 1);
+            tc::mbar_init(&sm.a_full[i], 256);
+            tc::mbar_init(&sm.mma_done[i], 1);
+            tc::mbar_init(&sm.d_empty[i], 128);
+            tc::mbar_init(&sm.m_full[i], 256);
+            tc::mbar_init(&sm.m_empty[i], 256);
+        }
+        tc::mbar_init(sm.d_full, 1);
+        *sm.abort = 0;
+        tc::fence_mbar_init();
+    }
+    if (warp == 0) tc::tmem_alloc(sm.tmem_base, 512);
+    for (int j = threadIdx.x; j < K; j += kThreads) {
+        sm.p_recip[j] = static_cast<float>(d.p_recip[j]);
+        sm.m_top[j] = d.M[static_cast<size_t>(j) * L + L - 1];
+    }
+    for (int k = threadIdx.x; k < kX; k += kThreads) sm.q[k] = k < L ? d.q[k] : 0u;
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *sm.tmem_base;
+
+    if (warp == 0) {
+        // ---- producer: y rows and constant chunks, two-slot rings ----
+        if (lane == 0) {
+            const uint32_t bbytes = U * 128;
+            uint32_t y_par[2] = {0, 0}, b_par[2] = {0, 0};   // parity of each slot's last arming
+            bool armed_y[2] = {false, false}, armed_b[2] = {false, false};
+            uint32_t g = 0;
+            for (uint32_t t = blockIdx.x; t < tiles && !*sm.abort; t += gridDim.x) {
+                const uint32_t n0 = n_begin + t * kSuper;
+                const uint32_t rows = min(kSuper, n_end - n0);
+                for (int c = 0; c < nch; ++c, ++g) {
+                    const int s = g & 1;
+                    if (g >= 2 && !wait_or_abort(&sm.y_empty[s], ((g - 2) >> 1) & 1, sm.abort)) break;
+                    const int j0 = c * kChunk, nj = max(0, min(static_cast<int>(kChunk), K - j0));
+                    tc::mbar_arrive_expect_tx(&sm.y_full[s], nj * rows * 4);
+                    for (int jj = 0; jj < nj; ++jj)
+                        tc::bulk_g2s(sm.yraw + s * kSlot + jj * kSuper * 4, Y + static_cast<size_t>(j0 + jj) * N + n0,
+                                     rows * 4, &sm.y_full[s]);
+                    y_par[s] = (g >> 1) & 1;
+                    armed_y[s] = true;
+                    if (g >= 2 && !wait_or_abort(&sm.mma_done[s], ((g - 2) >> 1) & 1, sm.abort)) break;
+                    tc::mbar_arrive_expect_tx(&sm.b_full[s], bbytes);
+                    tc::bulk_g2s(sm.b + s * kSlot, d.crt_img_v + static_cast<size_t>(c) * bbytes, bbytes,
+                                 &sm.b_full[s]);
+                    b_par[s] = (g >> 1) & 1;
+                    armed_b[s] = true;
+                }
+                if (*sm.abort) break;
+            }
+            // Copies still in flight must land before the CTA may exit.
+            for (int s = 0; s < 2; ++s) {
+                if (armed_y[s]) tc::wait_parity(&sm.y_full[s], y_par[s]);
+                if (armed_b[s]) tc::wait_parity(&sm.b_full[s], b_par[s]);
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ---- MMA issuer ----
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_u8(U);
+            uint32_t g = 0, it = 0;
+            bool issued = false;
+            uint32_t last_s = 0, last_par = 0;
+            for (uint32_t t = blockIdx.x; t < tiles && !*sm.abort; t += gridDim.x, ++it) {
+                bool ok = true;
+                if (it >= 1) {
+                    ok = wait_or_abort(&sm.d_empty[0], (it - 1) & 1, sm.abort) &&
+                         wait_or_abort(&sm.d_empty[1], (it - 1) & 1, sm.abort);
+                }
+                for (int c = 0; c < nch && ok; ++c, ++g) {
+                    const int s = g & 1;
+                    ok = wait_or_abort(&sm.b_full[s], (g >> 1) & 1, sm.abort) &&
+                         wait_or_abort(&sm.a_full[s], (g >> 1) & 1, sm.abort);
+                    if (!ok) break;
+                    tc::tc_fence_after();
+                    const uint32_t a0 = tc::smem_addr(sm.a + s * kSlot), b0 = tc::smem_addr(sm.b + s * kSlot);
+#pragma unroll
+                    for (uint32_t h = 0; h < 2; ++h) {
+#pragma unroll
+                        for (uint32_t kk = 0; kk < 4; ++kk) {
+                            const uint64_t ad = tc::smem_desc(a0 + h * 16384 + kk * 2 * 2048, 2048, 128);
+                            const uint64_t bd = tc::smem_desc(b0 + kk * 2 * (U * 16), U * 16, 128);
+                            tc::mma_u8(tmem + h * 256, ad, bd, idesc, c > 0 || kk > 0);
+                        }
+                    }
+                    tc::mma_commit(&sm.mma_done[s]);
+                    issued = true;
+                    last_s = s;
+                    last_par = (g >> 1) & 1;
+                }
+                if (!ok) break;
+                tc::mma_commit(sm.d_full);
+            }
+            // MMAs still running must finish before the CTA may exit.
+            if (issued) tc::wait_parity(&sm.mma_done[last_s], last_par);
+        }
+        __syncwarp();
+    } else if (warp < kEpiWarp0) {
+        // ---- stagers: thread = one row of the super-tile ----
+        const uint32_t row = threadIdx.x - kStagerWarp0 * 32;
+        const uint32_t h = row >> 7, m = row & 127;
+        uint32_t g = 0, it = 0;
+        for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+            const uint32_t n0 = n_begin + t * kSuper;
+            const bool live = row < min(kSuper, n_end - n0);
+            float frac0 = 0.f, frac1 = 0.f;
+            uint64_t tlo = 0, thi = 0;
+            bool ok = true;
+            for (int c = 0; c < nch; ++c, ++g) {
+                const int s = g & 1;
+                ok = wait_or_abort(&sm.y_full[s], (g >> 1) & 1, sm.abort);
+                if (ok && g >= 2) ok = wait_or_abort(&sm.mma_done[s], ((g - 2) >> 1) & 1, sm.abort);
+                ok = __all_sync(0xffffffffu, ok);
+                if (!ok) break;
+                const uint32_t* ys = reinterpret_cast<const uint32_t*>(sm.yraw + s * kSlot);
+                const int j0 = c * kChunk;
+                uint32_t yv[kChunk];
+#pragma unroll
+                for (int jj = 0; jj < static_cast<int>(kChunk); ++jj)
+                    yv[jj] = (live && j0 + jj < K) ? ys[jj * kSuper + row] : 0u;
+#pragma unroll
+                for (int jj = 0; jj < static_cast<int>(kChunk); ++jj) {
+                    const int j = j0 + jj;
+                    if (j < K) {
+                        const float f = static_cast<float>(yv[jj]) * sm.p_recip[j];
+                        if (jj & 1) {
+                            frac1 += f;
+                        } else {
+                            frac0 += f;
+                        }
+                        const uint64_t prod = static_cast<uint64_t>(yv[jj]) * sm.m_top[j];
+                        tlo += static_cast<uint32_t>(prod);
+                        thi += prod >> 32;
+                    }
+                }
+                if (c == nch - 1) {
+                    // Row K: the multiplier v of -P mod q.
+                    int v = __float2int_rn(frac0 + frac1);
+                    v = v < 0 ? 0 : (v > K ? K : v);
+                    if (!live) v = 0;
+                    const uint64_t prod = static_cast<uint64_t>(v) * d.negp_top;
+                    tlo += static_cast<uint32_t>(prod);
+                    thi += prod >> 32;
+#pragma unroll
+                    for (int jj = 0; jj < static_cast<int>(kChunk); ++jj)
+                        if (j0 + jj == K) yv[jj] = static_cast<uint32_t>(v);
+                }
+                uint8_t* as = sm.a + s * kSlot + h * 16384 + m * 16;
+#pragma unroll
+                for (int q4 = 0; q4 < 8; ++q4)
+                    *reinterpret_cast<uint4*>(as + q4 * 2048) =
+                        make_uint4(yv[4 * q4], yv[4 * q4 + 1], yv[4 * q4 + 2], yv[4 * q4 + 3]);
+                tc::fence_proxy_async_smem();
+                tc::mbar_arrive(&sm.a_full[s]);
+                tc::mbar_arrive(&sm.y_empty[s]);
+            }
+            if (!ok) break;
+            const int p = it & 1;
+            if (it >= 2) {
+                ok = wait_or_abort(&sm.m_empty[p], ((it - 2) >> 1) & 1, sm.abort);
+                ok = __all_sync(0xffffffffu, ok);
+                if (!ok) break;
+            }
+            const uint64_t t1 = (tlo >> 32) + thi;
+            sm.meta[p * kSuper + row] =
+                make_uint4(static_cast<uint32_t>(tlo), static_cast<uint32_t>(t1), static_cast<uint32_t>(t1 >> 32), 0u);
+            tc::mbar_arrive(&sm.m_full[p]);
+        }
+    } else {
+        // ---- epilogue: thread = one row of one half ----
+        const int ew = warp - kEpiWarp0;
+        const uint32_t h = ew >> 2, qd = warp & 3;
+        const uint32_t row = h * 128 + qd * 32 + lane;
+        const uint32_t tq = tmem + ((qd * 32) << 16) + h * 256;
+        const uint32_t npieces = U / 16;
+        const int n = L + 2, drop = top_drop(L);
+        const uint32_t top_piece = static_cast<uint32_t>(4 * drop) / 16;
+        const bool vec = (L & 3) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+        uint32_t it = 0;
+        for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
+            const uint32_t n0 = n_begin + t * kSuper;
+            const bool live = row < min(kSuper, n_end - n0);
+            const int p = it & 1;
+            bool ok = wait_or_abort(&sm.m_full[p], (it >> 1) & 1, sm.abort);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) break;
+            const uint4 meta = sm.meta[p * kSuper + row];
+            tc::mbar_arrive(&sm.m_empty[p]);
+            ok = wait_or_abort(sm.d_full, it & 1, sm.abort);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) break;
+            tc::tc_fence_after();
+            uint32_t rr[16];
+            // Quotient estimate from the columns at and above limb `drop` and the
+            // top-limb words: |estimate - X / q| < 2^-11, so e is within one.
+            double xd = 0;
+            for (uint32_t pc = npieces; pc-- > top_piece;) {
+                tmem_ld16_sync(tq + pc * 16, rr);
+#pragma unroll
+                for (int k = 15; k >= 0; --k) xd = xd * 256.0 + rr[k];
+            }
+            xd = ldexp(xd, static_cast<int>(8 * 16 * top_piece) - 32 * drop) +
+                 ldexp(static_cast<double>(meta.x), 32 * (L - 1 - drop)) +
+                 ldexp(static_cast<double>(meta.y), 32 * (L - drop)) +
+                 ldexp(static_cast<double>(meta.z), 32 * (L + 1 - drop));
+            const double f = floor(xd * d.q_top_inv);
+            const uint64_t e = f > 0 ? static_cast<uint64_t>(f) : 0;
+            const uint32_t e_lo = static_cast<uint32_t>(e), e_hi = static_cast<uint32_t>(e >> 32);
+            uint32_t* out = C + static_cast<size_t>(n0 + row) * L;
+            // One pass from the bottom: X with carries, minus e q; the borrows
+            // of X - e q (b0) and of (X - e q) - q (b1).
+            uint64_t carry = 0, c0 = 0;
+            uint32_t b0 = 0, b1 = 0;
+            uint32_t o[4];
+#pragma unroll
+            for (int k = 0; k < kX; ++k) {
+                const int i = k & 3;
+                if (i == 0) {
+                    if (k / 4 < 16 && static_cast<uint32_t>(k / 4) < npieces) {
+                        tmem_ld16_sync(tq + (k / 4) * 16, rr);
+                    } else {
+#pragma unroll
+                        for (int z = 0; z < 16; ++z) rr[z] = 0;
+                    }
+                }
+                if (k < n) {
+                    uint64_t w = carry + static_cast<uint64_t>(rr[4 * i]) + (static_cast<uint64_t>(rr[4 * i + 1]) << 8) +
+                                 (static_cast<uint64_t>(rr[4 * i + 2]) << 16) +
+                                 (static_cast<uint64_t>(rr[4 * i + 3]) << 24);
+                    if (k == L - 1) w += meta.x;
+                    if (k == L) w += meta.y;
+                    if (k == L + 1) w += meta.z;
+                    carry = w >> 32;
+                    const uint32_t qk = sm.q[k];
+                    const uint64_t acc = static_cast<uint64_t>(e_lo) * qk + c0;
+                    c0 = (acc >> 32) + static_cast<uint64_t>(e_hi) * qk;
+                    const uint64_t dy = static_cast<uint64_t>(static_cast<uint32_t>(w)) - static_cast<uint32_t>(acc) - b0;
+                    const uint32_t yk = static_cast<uint32_t>(dy);
+                    b0 = static_cast<uint32_t>(dy >> 63);
+                    b1 = static_cast<uint32_t>((static_cast<uint64_t>(yk) - qk - b1) >> 63);
+                    o[i] = yk;
+                    if (k < L && live) {
+                        if (vec) {
+                            if (i == 3) *reinterpret_cast<uint4*>(out + k - 3) = make_uint4(o[0], o[1], o[2], o[3]);
+                        } else {
+                            out[k] = yk;
+                        }
+                    }
+                }
+            }
+            // TMEM is read: the next super-tile's MMAs may start on this half.
+            tc::tc_fence_before();
+            tc::mbar_arrive(&sm.d_empty[h]);
+            // X - e q is negative (add q) or at least q (subtract q): rare.
+            if (live && (b0 || !b1)) {
+                uint32_t cb = 0;
+                for (int k = 0; k < L; ++k) {
+                    const uint32_t x = out[k], qk = sm.q[k];
+                    if (b0) {
+                        const uint64_t sum = static_cast<uint64_t>(x) + qk + cb;
+                        out[k] = static_cast<uint32_t>(sum);
+                        cb = static_cast<uint32_t>(sum >> 32);
+                    } else {
+                        const uint64_t dd = static_cast<uint64_t>(x) - qk - cb;
+                        out[k] = static_cast<uint32_t>(dd);
+                        cb = static_cast<uint32_t>(dd >> 63);
+                    }
+                }
+            }
+        }
+    }
+
+    tc::tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && *sm.abort) atomicOr(d.err, 2u);
+    if (warp == 0) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, 512);
+    }
+}
+
+}  // namespace
+
+bool crt_pipe_supported(const DevPoint& d, const uint32_t* Y, uint32_t n_begin, uint32_t n_end) {
+    // Bulk copies of y rows need 16-byte aligned starts and lengths.
+    return d.L >= 2 && d.crt_u <= 256 && d.K + 1 <= kMaxK && d.crt_img_v && (d.N & 3) == 0 && (n_begin & 3) == 0 &&
+           (n_end & 3) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15) == 0;
+}
+
+void crt_pipe_init_attributes() {
+    check(cudaFuncSetAttribute(k_crt_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemBytes)),
+          "crt_pipe smem");
+}
+
+void launch_crt_pipe(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_begin, uint32_t n_end, int sms,
+                     cudaStream_t st) {
+    if (n_end <= n_begin) return;
+    const uint32_t tiles = (n_end - n_begin + kSuper - 1) / kSuper;
+    const uint32_t grid = tiles < static_cast<uint32_t>(sms) ? tiles : static_cast<uint32_t>(sms);
+    k_crt_pipe<<<grid, kThreads, kSmemBytes, st>>>(d, Y, c, n_begin, n_end);
+}
+
+}  // namespace fpm

@@ -81,6 +81,7 @@ __device__ __forceinline__ void dec_body(const DevPoint& d, const uint32_t* __re
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int L = d.L;
 
+    const uint32_t chunk_bytes = kCols * kb;
     if (threadIdx.x == 0) {
         for (int i = 0; i < 2; ++i) {
             tc::mbar_init(&sm.full[i], 1);
@@ -88,6 +89,11 @@ __device__ __forceinline__ void dec_body(const DevPoint& d, const uint32_t* __re
             tc::mbar_init(&sm.tmem_empty[i], kEpi);
         }
         tc::fence_mbar_init();
+        // The first two constant chunks load under the operand tile's load.
+        for (int c = 0; c < (nch < 2 ? nch : 2); ++c) {
+            tc::mbar_arrive_expect_tx(&sm.full[c], chunk_bytes);
+            tc::bulk_g2s(sm.b0 + c * chunk_bytes, img + static_cast<size_t>(c) * chunk_bytes, chunk_bytes, &sm.full[c]);
+        }
     }
     if (warp == 0) tc::tmem_alloc(sm.tmem_base, 2 * kCols);
     for (int j = threadIdx.x; j < d.K; j += kThreads) sm.fold[j] = d.dec_fold[j];
@@ -151,12 +157,6 @@ __device__ __forceinline__ void dec_body(const DevPoint& d, const uint32_t* __re
 
     if (warp == 0) {
         if (lane == 0) {
-            const uint32_t chunk_bytes = kCols * kb;
-            const int pre = nch < 2 ? nch : 2;
-            for (int c = 0; c < pre; ++c) {
-                tc::mbar_arrive_expect_tx(&sm.full[c], chunk_bytes);
-                tc::bulk_g2s(sm.b0 + c * chunk_bytes, img + static_cast<size_t>(c) * chunk_bytes, chunk_bytes, &sm.full[c]);
-            }
             const uint32_t idesc = tc::idesc_u8(kCols);
             const uint32_t a0 = tc::smem_addr(sm.a);
             for (int c = 0; c < nch && ok; ++c) {
@@ -236,11 +236,15 @@ __device__ __forceinline__ void dec_body(const DevPoint& d, const uint32_t* __re
     }
 }
 
+// Grid (tiles, operands): blockIdx.y = 1 takes the second operand (lb, rb).
 __global__ void __launch_bounds__(kThreads)
-    k_decompose_tc(DevPoint d, const uint32_t* __restrict__ limbs, uint32_t* __restrict__ res, int operand,
-                   uint32_t n_begin, uint32_t n_end) {
+    k_decompose_tc(DevPoint d, const uint32_t* __restrict__ la, const uint32_t* __restrict__ lb,
+                   uint32_t* __restrict__ ra, uint32_t* __restrict__ rb, int operand0, uint32_t n_begin,
+                   uint32_t n_end) {
     const uint32_t n0 = n_begin + blockIdx.x * kRows;
-    dec_body(d, limbs, res, operand, n0, min(kRows, n_end - n0));
+    const bool second = blockIdx.y != 0;
+    dec_body(d, second ? lb : la, second ? rb : ra, operand0 + static_cast<int>(blockIdx.y), n0,
+             min(kRows, n_end - n0));
 }
 
 // Grouped: item i owns 2 ceil(N / 128) blocks, operand a's tiles then b's.
@@ -282,7 +286,14 @@ void launch_decompose_tc(const DevPoint& d, const uint32_t* limbs, uint32_t* res
                          uint32_t n_end, cudaStream_t st) {
     if (n_end <= n_begin) return;
     const uint32_t blocks = (n_end - n_begin + kRows - 1) / kRows;
-    k_decompose_tc<<<blocks, kThreads, smem_bytes(d.dec_kb), st>>>(d, limbs, res, operand, n_begin, n_end);
+    k_decompose_tc<<<blocks, kThreads, smem_bytes(d.dec_kb), st>>>(d, limbs, limbs, res, res, operand, n_begin,
+                                                                    n_end);
+}
+
+void launch_decompose_tc_pair(const DevPoint& d, const uint32_t* a, const uint32_t* b, uint32_t* A, uint32_t* B,
+                              cudaStream_t st) {
+    const dim3 grid((d.N + kRows - 1) / kRows, 2);
+    k_decompose_tc<<<grid, kThreads, smem_bytes(d.dec_kb), st>>>(d, a, b, A, B, 0, 0, d.N);
 }
 
 }  // namespace fpm

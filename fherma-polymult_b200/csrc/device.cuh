@@ -24,6 +24,7 @@ struct DevPoint {
     const uint2* full_i;
     const uint32_t* q;         // L
     double q_top;
+    double q_top_inv;          // 1 / q_top, for the quotient estimate
     const uint32_t* M;         // K x L
     const uint32_t* negvP;     // (K + 1) x L
     const double* p_recip;     // K
@@ -37,6 +38,8 @@ struct DevPoint {
     uint32_t crt_u;
     uint32_t crt_tmem_cols;
     const uint8_t* crt_img;
+    const uint8_t* crt_img_v;  // K + 1 rows: row K is -P mod q (pipelined CRT)
+    uint32_t negp_top;         // (-P mod q)'s top limb
     // error word: bit 0 decompose, bit 1 CRT (a pipeline wait timed out)
     uint32_t* err;
 };

@@ -28,6 +28,7 @@ void ensure_kernel_attributes(int device) {
     crt_init_attributes();
     decompose_tc_init_attributes();
     crt_tc_init_attributes();
+    crt_pipe_init_attributes();
     done.push_back(device);
 }
 
@@ -51,6 +52,7 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
     : plan_(make_plan(N, W, q, L, pmax_log2)) {
     try {
         check(cudaGetDevice(&device_), "cudaGetDevice");
+        check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_), "SM count");
         ensure_kernel_attributes(device_);
         const HostPlan& pl = plan_;
         dp_.N = pl.N;
@@ -71,6 +73,7 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
         dp_.full_i = upload(pl.full_i);
         dp_.q = upload(pl.q);
         dp_.q_top = pl.q_top;
+        dp_.q_top_inv = 1.0 / pl.q_top;
         dp_.M = upload(pl.M);
         dp_.negvP = upload(pl.negvP);
         dp_.p_recip = upload(pl.p_recip);
@@ -82,6 +85,8 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
         dp_.crt_u = pl.crt_u;
         dp_.crt_tmem_cols = pl.crt_tmem_cols;
         dp_.crt_img = upload(pl.crt_img);
+        dp_.crt_img_v = upload(pl.crt_img_v);
+        dp_.negp_top = pl.negp_top;
         dp_.err = dalloc<uint32_t>(1);
         check(cudaMemset(dp_.err, 0, sizeof(uint32_t)), "memset");
         if (const char* k = std::getenv("FPM_KERNELS")) simt_ = std::strcmp(k, "simt") == 0;
@@ -129,6 +134,8 @@ void Engine::launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, u
 void Engine::launch_crt_any(const uint32_t* d_y, uint32_t* d_c, uint32_t n0, uint32_t n1, cudaStream_t st) {
     if (simt_ || !crt_uses_tc(plan_)) {
         launch_crt(dp_, d_y, d_c, n0, n1, st);
+    } else if (crt_pipe_supported(dp_, d_y, n0, n1)) {
+        launch_crt_pipe(dp_, d_y, d_c, n0, n1, sms_, st);
     } else {
         launch_crt_tc(dp_, d_y, d_c, n0, n1, st);
     }
@@ -157,8 +164,12 @@ void Engine::crt(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st) {
 }
 
 void Engine::run_device(const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t st) {
-    launch_dec(d_a, A_, 0, 0, plan_.N, st);
-    launch_dec(d_b, B_, 1, 0, plan_.N, st);
+    if (simt_) {
+        launch_dec(d_a, A_, 0, 0, plan_.N, st);
+        launch_dec(d_b, B_, 1, 0, plan_.N, st);
+    } else {
+        launch_decompose_tc_pair(dp_, d_a, d_b, A_, B_, st);
+    }
     launch_ntt(dp_, A_, B_, kRowProduct, st);
     launch_crt_any(A_, d_c, 0, plan_.N, st);
     check(cudaGetLastError(), "product launch");

@@ -76,6 +76,7 @@ private:
     HostPlan plan_;
     DevPoint dp_{};
     int device_ = 0;
+    int sms_ = 0;
     bool simt_ = false;        // FPM_KERNELS=simt: CUDA-core decompose and CRT
     std::vector<void*> dmem_;
     uint32_t* A_ = nullptr;   // K x N residues

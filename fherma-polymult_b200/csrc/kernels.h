@@ -51,11 +51,22 @@ void launch_ntt(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStrea
 void launch_decompose_tc(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, uint32_t n_begin,
                          uint32_t n_end, cudaStream_t st);
 
+// Both operands of a product in one launch: a -> A (operand 0), b -> B (1).
+void launch_decompose_tc_pair(const DevPoint& d, const uint32_t* a, const uint32_t* b, uint32_t* A, uint32_t* B,
+                              cudaStream_t st);
+
 // y_j (K x N) -> c (N x L) mod q: CUDA cores, and tensor cores (L >= 2).
 void launch_crt(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_begin, uint32_t n_end,
                 cudaStream_t st);
 void launch_crt_tc(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_begin, uint32_t n_end,
                    cudaStream_t st);
+
+// The persistent CRT pipeline (crt_pipe.cu): one CTA per SM, `sms` at most.
+// Needs L >= 2 and N, n_begin, n_end multiples of 4.
+bool crt_pipe_supported(const DevPoint& d, const uint32_t* Y, uint32_t n_begin, uint32_t n_end);
+void crt_pipe_init_attributes();
+void launch_crt_pipe(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_begin, uint32_t n_end, int sms,
+                     cudaStream_t st);
 
 // Grouped launches (group.cuh): one launch covers every item of the table,
 // whose first[] the caller fills with these per-item block counts.

@@ -97,7 +97,7 @@ size_t device_footprint(const HostPlan& pl) {
                bytes(pl.row_u_f) + bytes(pl.row_q_f) +
                bytes(pl.full_f) + bytes(pl.full_i) + bytes(pl.q) + bytes(pl.M) + bytes(pl.negvP) +
                bytes(pl.p_recip) + bytes(pl.dec_img_a) + bytes(pl.dec_img_b) + bytes(pl.dec_fold) +
-               bytes(pl.crt_img) + sizeof(uint32_t);
+               bytes(pl.crt_img) + bytes(pl.crt_img_v) + sizeof(uint32_t);
     t += 2 * static_cast<size_t>(pl.K) * pl.N * sizeof(uint32_t);   // residue workspaces
     t += 3 * static_cast<size_t>(pl.N) * pl.L * sizeof(uint32_t);   // host-path limb buffers
     return t;
@@ -292,19 +292,30 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
         const uint32_t chunks = static_cast<uint32_t>((K + 31) / 32);
         const size_t cchunk = static_cast<size_t>(pl.crt_u) * 128;
         const uint32_t low_bytes = 4 * static_cast<uint32_t>(L - 1);
-        pl.crt_img.assign(cchunk * chunks, 0);
-        for (int j = 0; j < K; ++j) {
-            const uint32_t* m = &pl.M[static_cast<size_t>(j) * L];
-            for (int s = 0; s < 4; ++s) {
-                const uint32_t kbyte = 4 * (j % 32) + s;   // K index within the chunk
-                for (uint32_t u = s; u < pl.crt_u && u - s < low_bytes; ++u) {
-                    const uint32_t byte = u - s;
-                    const size_t at = static_cast<size_t>(j / 32) * cchunk + (kbyte / 16) * (pl.crt_u * 16) +
-                                      u * 16 + (kbyte % 16);
-                    pl.crt_img[at] = static_cast<uint8_t>(m[byte / 4] >> (8 * (byte % 4)));
+        // Row j of an image holds the byte shifts of constant j's low L - 1 limbs.
+        auto build = [&](std::vector<uint8_t>& img, int rows, auto&& limbs_of) {
+            img.assign(cchunk * static_cast<size_t>((rows + 31) / 32), 0);
+            for (int j = 0; j < rows; ++j) {
+                const uint32_t* m = limbs_of(j);
+                for (int s = 0; s < 4; ++s) {
+                    const uint32_t kbyte = 4 * (j % 32) + s;   // K index within the chunk
+                    for (uint32_t u = s; u < pl.crt_u && u - s < low_bytes; ++u) {
+                        const uint32_t byte = u - s;
+                        const size_t at = static_cast<size_t>(j / 32) * cchunk + (kbyte / 16) * (pl.crt_u * 16) +
+                                          u * 16 + (kbyte % 16);
+                        img[at] = static_cast<uint8_t>(m[byte / 4] >> (8 * (byte % 4)));
+                    }
                 }
             }
-        }
+        };
+        (void)chunks;
+        build(pl.crt_img, K, [&](int j) { return &pl.M[static_cast<size_t>(j) * L]; });
+        // The same with one more row, -P mod q: its multiplier is v, so the
+        // GEMM itself adds -v P (the pipelined CRT needs no negvP table).
+        build(pl.crt_img_v, K + 1, [&](int j) {
+            return j < K ? &pl.M[static_cast<size_t>(j) * L] : &pl.negvP[static_cast<size_t>(L)];
+        });
+        pl.negp_top = pl.negvP[static_cast<size_t>(L) + L - 1];
     }
     return pl;
 }

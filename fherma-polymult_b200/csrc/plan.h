@@ -87,6 +87,10 @@ struct HostPlan {
     uint32_t crt_u = 0;
     uint32_t crt_tmem_cols = 0;              // power of two >= crt_u
     std::vector<uint8_t> crt_img;
+    // The same image with a row K for -P mod q (= negvP_1), and that
+    // constant's top limb: the pipelined CRT multiplies it by v in the GEMM.
+    std::vector<uint8_t> crt_img_v;
+    uint32_t negp_top = 0;
 };
 
 // Which CRT kernel the point uses: the tensor-core one needs L >= 2.
