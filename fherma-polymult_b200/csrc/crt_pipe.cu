@@ -9,9 +9,9 @@
 //
 // The low L - 1 limbs of every constant go through the 8-bit GEMM
 // D[m][u] = sum_{j,s} byte_s(y_j(m)) byte_{u-s}(Mlow_j) (entries < 2^26); the
-// top limb sum_j y_j M_j[L-1] and the rounding sum run on the CUDA cores.  The
-// rounding sum is within 2^-20 of an integer (the prime basis covers 2^20 N q^2),
-// so single precision decides v.
+// top limb and the rounding sum run on the CUDA cores.  The prime basis covers
+// 2^20 N q^2, so sum_j y_j / p_j lies within 2^-21 of an integer and a
+// fixed-point sum with r_j = floor(2^50 / p_j) (error below 2^-11) rounds to v.
 //
 // Organisation on the B200:
 //   * one CTA per SM walks super-tiles of 256 coefficients; TMEM's 512 columns
@@ -29,6 +29,10 @@
 //     limbs and tracks the borrows that tell whether X - e q lies in [0, q);
 //     the rare row that does not (about 2^-11 of them) adds or subtracts q in
 //     a second pass over what it stored.
+// Per-prime constants and q come from kernel parameters (constant bank), so
+// shared memory carries only y, the MMA operands and the per-row top limbs.
+// The kernel is compiled for the common limb counts (L = 64, 55, 28, 8) and
+// once for any L.
 //
 // Every wait is bounded; a timeout raises an abort flag that every role
 // checks, the producer and the MMA thread wait out what they have in flight,
@@ -46,6 +50,7 @@ constexpr int kStagerWarp0 = 2;           // warps 2-9
 constexpr int kEpiWarp0 = 10;             // warps 10-17
 constexpr uint32_t kSuper = 256;          // coefficients per super-tile
 constexpr uint32_t kChunk = 32;           // K rows (primes) per chunk
+constexpr int kMaxChunks = kMaxK / kChunk;   // K + 1 <= kMaxK rows
 constexpr uint32_t kSlot = 32768;         // bytes: y slot, A slot (two halves), B slot (U <= 256)
 constexpr int kX = kMaxL + 2;
 
@@ -54,9 +59,6 @@ struct Smem {
     uint8_t* a;          // [2][2 halves][16 KB]
     uint8_t* b;          // [2][U x 128]
     uint4* meta;         // [2][256] {top limb words 0, 1, 2, -}
-    float* p_recip;      // [kMaxK]
-    uint32_t* m_top;     // [kMaxK]
-    uint32_t* q;         // [kX]: q, zero above L
     uint64_t* y_full;    // [2]
     uint64_t* y_empty;   // [2]
     uint64_t* b_full;    // [2]
@@ -71,9 +73,8 @@ struct Smem {
 };
 
 constexpr size_t kMetaOff = 6 * size_t(kSlot);
-constexpr size_t kConstOff = kMetaOff + 2 * kSuper * sizeof(uint4);
-constexpr size_t kBarOff = kConstOff + kMaxK * 4 + kMaxK * 4 + kX * 4;
-constexpr size_t kSmemBytes = ((kBarOff + 7) / 8) * 8 + 17 * 8 + 16;
+constexpr size_t kBarOff = kMetaOff + 2 * kSuper * sizeof(uint4);
+constexpr size_t kSmemBytes = kBarOff + 17 * 8 + 16;
 
 __device__ inline Smem carve(uint8_t* base) {
     Smem s;
@@ -81,10 +82,7 @@ __device__ inline Smem carve(uint8_t* base) {
     s.a = base + 2 * kSlot;
     s.b = base + 4 * kSlot;
     s.meta = reinterpret_cast<uint4*>(base + kMetaOff);
-    s.p_recip = reinterpret_cast<float*>(base + kConstOff);
-    s.m_top = reinterpret_cast<uint32_t*>(s.p_recip + kMaxK);
-    s.q = s.m_top + kMaxK;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(base + ((kBarOff + 7) / 8) * 8);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + kBarOff);
     s.y_full = bars;
     s.y_empty = bars + 2;
     s.b_full = bars + 4;
@@ -113,9 +111,9 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, vo
     return true;
 }
 
-// 16 TMEM columns; the wait names the registers so no read moves above it.
-__device__ __forceinline__ void tmem_ld16_sync(uint32_t taddr, uint32_t (&r)[16]) {
-    tc::tmem_ld16(taddr, r);
+// Waits for this thread's TMEM loads; naming the registers keeps every read of
+// them below the wait.
+__device__ __forceinline__ void tmem_wait(uint32_t (&r)[16]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;"
                  : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
                    "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
@@ -124,14 +122,17 @@ __device__ __forceinline__ void tmem_ld16_sync(uint32_t taddr, uint32_t (&r)[16]
                  : "memory");
 }
 
+// LT > 0: L = LT at compile time; LT = 0: any L (predicated).
+template <int LT>
 __global__ void __launch_bounds__(kThreads, 1)
-    k_crt_pipe(DevPoint d, const uint32_t* __restrict__ Y, uint32_t* __restrict__ C, uint32_t n_begin,
-               uint32_t n_end) {
+    k_crt_pipe(DevPoint d, const __grid_constant__ CrtConsts cc, const uint32_t* __restrict__ Y,
+               uint32_t* __restrict__ C, uint32_t n_begin, uint32_t n_end) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     const Smem sm = carve(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int L = d.L, K = d.K;
-    const uint32_t U = d.crt_u;
+    const int L = LT > 0 ? LT : d.L;
+    const int K = d.K;
+    const uint32_t U = LT > 0 ? (4 * LT - 1 + 31) / 32 * 32 : d.crt_u;
     const uint32_t N = d.N;
     const int nch = (K + 1 + static_cast<int>(kChunk) - 1) / static_cast<int>(kChunk);   // K + 1 rows
     const uint32_t tiles = (n_end - n_begin + kSuper - 1) / kSuper;
@@ -152,11 +153,6 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc::fence_mbar_init();
     }
     if (warp == 0) tc::tmem_alloc(sm.tmem_base, 512);
-    for (int j = threadIdx.x; j < K; j += kThreads) {
-        sm.p_recip[j] = static_cast<float>(d.p_recip[j]);
-        sm.m_top[j] = d.M[static_cast<size_t>(j) * L + L - 1];
-    }
-    for (int k = threadIdx.x; k < kX; k += kThreads) sm.q[k] = k < L ? d.q[k] : 0u;
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
@@ -218,10 +214,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                     if (!ok) break;
                     tc::tc_fence_after();
                     const uint32_t a0 = tc::smem_addr(sm.a + s * kSlot), b0 = tc::smem_addr(sm.b + s * kSlot);
-#pragma unroll
+                    // K steps of 8 rows; the last chunk stops after row K.
+                    const int rows_c = min(static_cast<int>(kChunk), K + 1 - c * static_cast<int>(kChunk));
+                    const uint32_t ksteps = static_cast<uint32_t>(rows_c + 7) / 8;
                     for (uint32_t h = 0; h < 2; ++h) {
-#pragma unroll
-                        for (uint32_t kk = 0; kk < 4; ++kk) {
+                        for (uint32_t kk = 0; kk < ksteps; ++kk) {
                             const uint64_t ad = tc::smem_desc(a0 + h * 16384 + kk * 2 * 2048, 2048, 128);
                             const uint64_t bd = tc::smem_desc(b0 + kk * 2 * (U * 16), U * 16, 128);
                             tc::mma_u8(tmem + h * 256, ad, bd, idesc, c > 0 || kk > 0);
@@ -247,47 +244,40 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
             const uint32_t n0 = n_begin + t * kSuper;
             const bool live = row < min(kSuper, n_end - n0);
-            float frac0 = 0.f, frac1 = 0.f;
-            uint64_t tlo = 0, thi = 0;
+            uint64_t vacc = 0, tlo = 0, thi = 0;   // sum y r50; sum y (top & 0xFFFF); sum y (top >> 16)
             bool ok = true;
-            for (int c = 0; c < nch; ++c, ++g) {
+#pragma unroll
+            for (int c = 0; c < kMaxChunks; ++c) {
+                if (c >= nch) break;
                 const int s = g & 1;
                 ok = wait_or_abort(&sm.y_full[s], (g >> 1) & 1, sm.abort);
                 if (ok && g >= 2) ok = wait_or_abort(&sm.mma_done[s], ((g - 2) >> 1) & 1, sm.abort);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
                 const uint32_t* ys = reinterpret_cast<const uint32_t*>(sm.yraw + s * kSlot);
-                const int j0 = c * kChunk;
                 uint32_t yv[kChunk];
 #pragma unroll
                 for (int jj = 0; jj < static_cast<int>(kChunk); ++jj)
-                    yv[jj] = (live && j0 + jj < K) ? ys[jj * kSuper + row] : 0u;
+                    yv[jj] = (live && c * static_cast<int>(kChunk) + jj < K) ? ys[jj * kSuper + row] : 0u;
 #pragma unroll
                 for (int jj = 0; jj < static_cast<int>(kChunk); ++jj) {
-                    const int j = j0 + jj;
+                    const int j = c * static_cast<int>(kChunk) + jj;
                     if (j < K) {
-                        const float f = static_cast<float>(yv[jj]) * sm.p_recip[j];
-                        if (jj & 1) {
-                            frac1 += f;
-                        } else {
-                            frac0 += f;
-                        }
-                        const uint64_t prod = static_cast<uint64_t>(yv[jj]) * sm.m_top[j];
-                        tlo += static_cast<uint32_t>(prod);
-                        thi += prod >> 32;
+                        vacc += static_cast<uint64_t>(yv[jj]) * cc.r50[j];
+                        tlo += static_cast<uint64_t>(yv[jj]) * cc.mlo[j];
+                        thi += static_cast<uint64_t>(yv[jj]) * cc.mhi[j];
                     }
                 }
                 if (c == nch - 1) {
                     // Row K: the multiplier v of -P mod q.
-                    int v = __float2int_rn(frac0 + frac1);
-                    v = v < 0 ? 0 : (v > K ? K : v);
-                    if (!live) v = 0;
-                    const uint64_t prod = static_cast<uint64_t>(v) * d.negp_top;
-                    tlo += static_cast<uint32_t>(prod);
-                    thi += prod >> 32;
+                    int v = static_cast<int>((vacc + (1ull << 49)) >> 50);
+                    v = v > K ? K : v;
+                    const uint32_t vu = live ? static_cast<uint32_t>(v) : 0u;
+                    tlo += static_cast<uint64_t>(vu) * cc.mlo[K];
+                    thi += static_cast<uint64_t>(vu) * cc.mhi[K];
 #pragma unroll
                     for (int jj = 0; jj < static_cast<int>(kChunk); ++jj)
-                        if (j0 + jj == K) yv[jj] = static_cast<uint32_t>(v);
+                        if (c * static_cast<int>(kChunk) + jj == K) yv[jj] = vu;
                 }
                 uint8_t* as = sm.a + s * kSlot + h * 16384 + m * 16;
 #pragma unroll
@@ -297,6 +287,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tc::fence_proxy_async_smem();
                 tc::mbar_arrive(&sm.a_full[s]);
                 tc::mbar_arrive(&sm.y_empty[s]);
+                ++g;
             }
             if (!ok) break;
             const int p = it & 1;
@@ -305,9 +296,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
             }
-            const uint64_t t1 = (tlo >> 32) + thi;
+            // Top-limb sum = tlo + thi 2^16, as three words.
+            const uint64_t t0 = tlo + ((thi & 0xFFFFu) << 16);
+            const uint64_t t1 = (t0 >> 32) + (thi >> 16);
             sm.meta[p * kSuper + row] =
-                make_uint4(static_cast<uint32_t>(tlo), static_cast<uint32_t>(t1), static_cast<uint32_t>(t1 >> 32), 0u);
+                make_uint4(static_cast<uint32_t>(t0), static_cast<uint32_t>(t1), static_cast<uint32_t>(t1 >> 32), 0u);
             tc::mbar_arrive(&sm.m_full[p]);
         }
     } else {
@@ -320,6 +313,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int n = L + 2, drop = top_drop(L);
         const uint32_t top_piece = static_cast<uint32_t>(4 * drop) / 16;
         const bool vec = (L & 3) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+        constexpr int kXL = LT > 0 ? LT + 2 : kX;        // limbs handled
+        constexpr int kPieces = (kXL + 3) / 4;
         uint32_t it = 0;
         for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
             const uint32_t n0 = n_begin + t * kSuper;
@@ -334,14 +329,15 @@ __global__ void __launch_bounds__(kThreads, 1)
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) break;
             tc::tc_fence_after();
-            uint32_t rr[16];
+            uint32_t ra[16], rb[16];
             // Quotient estimate from the columns at and above limb `drop` and the
             // top-limb words: |estimate - X / q| < 2^-11, so e is within one.
             double xd = 0;
             for (uint32_t pc = npieces; pc-- > top_piece;) {
-                tmem_ld16_sync(tq + pc * 16, rr);
+                tc::tmem_ld16(tq + pc * 16, ra);
+                tmem_wait(ra);
 #pragma unroll
-                for (int k = 15; k >= 0; --k) xd = xd * 256.0 + rr[k];
+                for (int k = 15; k >= 0; --k) xd = xd * 256.0 + ra[k];
             }
             xd = ldexp(xd, static_cast<int>(8 * 16 * top_piece) - 32 * drop) +
                  ldexp(static_cast<double>(meta.x), 32 * (L - 1 - drop)) +
@@ -352,45 +348,54 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t e_lo = static_cast<uint32_t>(e), e_hi = static_cast<uint32_t>(e >> 32);
             uint32_t* out = C + static_cast<size_t>(n0 + row) * L;
             // One pass from the bottom: X with carries, minus e q; the borrows
-            // of X - e q (b0) and of (X - e q) - q (b1).
+            // of X - e q (b0) and of (X - e q) - q (b1).  TMEM pieces are
+            // double-buffered: piece pc + 1 loads while piece pc is used.
             uint64_t carry = 0, c0 = 0;
             uint32_t b0 = 0, b1 = 0;
             uint32_t o[4];
+            tc::tmem_ld16(tq, ra);
+            tmem_wait(ra);
 #pragma unroll
-            for (int k = 0; k < kX; ++k) {
-                const int i = k & 3;
-                if (i == 0) {
-                    if (k / 4 < 16 && static_cast<uint32_t>(k / 4) < npieces) {
-                        tmem_ld16_sync(tq + (k / 4) * 16, rr);
-                    } else {
+            for (int pc = 0; pc < kPieces; ++pc) {
+                uint32_t(&cur)[16] = (pc & 1) ? rb : ra;
+                uint32_t(&nxt)[16] = (pc & 1) ? ra : rb;
+                const bool have = static_cast<uint32_t>(pc) < npieces;
+                const bool more = static_cast<uint32_t>(pc + 1) < npieces;
+                if (more) tc::tmem_ld16(tq + (pc + 1) * 16, nxt);
 #pragma unroll
-                        for (int z = 0; z < 16; ++z) rr[z] = 0;
-                    }
-                }
-                if (k < n) {
-                    uint64_t w = carry + static_cast<uint64_t>(rr[4 * i]) + (static_cast<uint64_t>(rr[4 * i + 1]) << 8) +
-                                 (static_cast<uint64_t>(rr[4 * i + 2]) << 16) +
-                                 (static_cast<uint64_t>(rr[4 * i + 3]) << 24);
-                    if (k == L - 1) w += meta.x;
-                    if (k == L) w += meta.y;
-                    if (k == L + 1) w += meta.z;
-                    carry = w >> 32;
-                    const uint32_t qk = sm.q[k];
-                    const uint64_t acc = static_cast<uint64_t>(e_lo) * qk + c0;
-                    c0 = (acc >> 32) + static_cast<uint64_t>(e_hi) * qk;
-                    const uint64_t dy = static_cast<uint64_t>(static_cast<uint32_t>(w)) - static_cast<uint32_t>(acc) - b0;
-                    const uint32_t yk = static_cast<uint32_t>(dy);
-                    b0 = static_cast<uint32_t>(dy >> 63);
-                    b1 = static_cast<uint32_t>((static_cast<uint64_t>(yk) - qk - b1) >> 63);
-                    o[i] = yk;
-                    if (k < L && live) {
-                        if (vec) {
-                            if (i == 3) *reinterpret_cast<uint4*>(out + k - 3) = make_uint4(o[0], o[1], o[2], o[3]);
-                        } else {
-                            out[k] = yk;
+                for (int i = 0; i < 4; ++i) {
+                    const int k = 4 * pc + i;
+                    if (k < kXL && k < n) {
+                        uint64_t w = carry;
+                        if (have) {
+                            w += cur[4 * i];
+                            w += static_cast<uint64_t>(cur[4 * i + 1]) * 256u;
+                            w += static_cast<uint64_t>(cur[4 * i + 2]) * 65536u;
+                            w += static_cast<uint64_t>(cur[4 * i + 3]) * 16777216u;
+                        }
+                        if (k == L - 1) w += meta.x;
+                        if (k == L) w += meta.y;
+                        if (k == L + 1) w += meta.z;
+                        carry = w >> 32;
+                        const uint32_t qk = cc.q[k];
+                        const uint64_t acc = static_cast<uint64_t>(e_lo) * qk + c0;
+                        c0 = (acc >> 32) + static_cast<uint64_t>(e_hi) * qk;
+                        const uint64_t dy =
+                            static_cast<uint64_t>(static_cast<uint32_t>(w)) - static_cast<uint32_t>(acc) - b0;
+                        const uint32_t yk = static_cast<uint32_t>(dy);
+                        b0 = static_cast<uint32_t>(dy >> 63);
+                        b1 = static_cast<uint32_t>((static_cast<uint64_t>(yk) - qk - b1) >> 63);
+                        o[i] = yk;
+                        if (k < L && live) {
+                            if (vec) {
+                                if (i == 3) *reinterpret_cast<uint4*>(out + k - 3) = make_uint4(o[0], o[1], o[2], o[3]);
+                            } else {
+                                out[k] = yk;
+                            }
                         }
                     }
                 }
+                if (more) tmem_wait(nxt);
             }
             // TMEM is read: the next super-tile's MMAs may start on this half.
             tc::tc_fence_before();
@@ -399,7 +404,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (live && (b0 || !b1)) {
                 uint32_t cb = 0;
                 for (int k = 0; k < L; ++k) {
-                    const uint32_t x = out[k], qk = sm.q[k];
+                    const uint32_t x = out[k], qk = cc.q[k];
                     if (b0) {
                         const uint64_t sum = static_cast<uint64_t>(x) + qk + cb;
                         out[k] = static_cast<uint32_t>(sum);
@@ -423,25 +428,55 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-}  // namespace
-
-bool crt_pipe_supported(const DevPoint& d, const uint32_t* Y, uint32_t n_begin, uint32_t n_end) {
-    // Bulk copies of y rows need 16-byte aligned starts and lengths.
-    return d.L >= 2 && d.crt_u <= 256 && d.K + 1 <= kMaxK && d.crt_img_v && (d.N & 3) == 0 && (n_begin & 3) == 0 &&
-           (n_end & 3) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15) == 0;
-}
-
-void crt_pipe_init_attributes() {
-    check(cudaFuncSetAttribute(k_crt_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kSmemBytes)),
+template <int LT>
+void set_attr() {
+    check(cudaFuncSetAttribute(k_crt_pipe<LT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(kSmemBytes)),
           "crt_pipe smem");
 }
 
-void launch_crt_pipe(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_begin, uint32_t n_end, int sms,
-                     cudaStream_t st) {
+}  // namespace
+
+CrtConsts make_crt_consts(const HostPlan& pl) {
+    CrtConsts cc{};
+    for (int j = 0; j < pl.K; ++j) {
+        cc.r50[j] = static_cast<uint32_t>((1ull << 50) / pl.primes[j]);
+        const uint32_t top = pl.M[static_cast<size_t>(j) * pl.L + pl.L - 1];
+        cc.mlo[j] = top & 0xFFFFu;
+        cc.mhi[j] = top >> 16;
+    }
+    cc.mlo[pl.K] = pl.negp_top & 0xFFFFu;
+    cc.mhi[pl.K] = pl.negp_top >> 16;
+    for (int k = 0; k < pl.L; ++k) cc.q[k] = pl.q[k];
+    return cc;
+}
+
+bool crt_pipe_supported(const DevPoint& d, const uint32_t* Y, uint32_t n_begin, uint32_t n_end) {
+    // Bulk copies of y rows need 16-byte aligned starts and lengths.
+    return d.L >= 2 && d.crt_u <= 256 && d.K + 1 <= kMaxK && d.crt_img_v && (d.N & 3) == 0 &&
+           (n_begin & 3) == 0 && (n_end & 3) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15) == 0;
+}
+
+void crt_pipe_init_attributes() {
+    set_attr<0>();
+    set_attr<64>();
+    set_attr<55>();
+    set_attr<28>();
+    set_attr<8>();
+}
+
+void launch_crt_pipe(const DevPoint& d, const CrtConsts& cc, const uint32_t* Y, uint32_t* c, uint32_t n_begin,
+                     uint32_t n_end, int sms, cudaStream_t st) {
     if (n_end <= n_begin) return;
     const uint32_t tiles = (n_end - n_begin + kSuper - 1) / kSuper;
     const uint32_t grid = tiles < static_cast<uint32_t>(sms) ? tiles : static_cast<uint32_t>(sms);
-    k_crt_pipe<<<grid, kThreads, kSmemBytes, st>>>(d, Y, c, n_begin, n_end);
+    switch (d.L) {
+        case 64: k_crt_pipe<64><<<grid, kThreads, kSmemBytes, st>>>(d, cc, Y, c, n_begin, n_end); break;
+        case 55: k_crt_pipe<55><<<grid, kThreads, kSmemBytes, st>>>(d, cc, Y, c, n_begin, n_end); break;
+        case 28: k_crt_pipe<28><<<grid, kThreads, kSmemBytes, st>>>(d, cc, Y, c, n_begin, n_end); break;
+        case 8: k_crt_pipe<8><<<grid, kThreads, kSmemBytes, st>>>(d, cc, Y, c, n_begin, n_end); break;
+        default: k_crt_pipe<0><<<grid, kThreads, kSmemBytes, st>>>(d, cc, Y, c, n_begin, n_end); break;
+    }
 }
 
 }  // namespace fpm

@@ -87,6 +87,7 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
         dp_.crt_img = upload(pl.crt_img);
         dp_.crt_img_v = upload(pl.crt_img_v);
         dp_.negp_top = pl.negp_top;
+        if (crt_uses_tc(pl)) crt_consts_.reset(new CrtConsts(make_crt_consts(pl)));
         dp_.err = dalloc<uint32_t>(1);
         check(cudaMemset(dp_.err, 0, sizeof(uint32_t)), "memset");
         if (const char* k = std::getenv("FPM_KERNELS")) simt_ = std::strcmp(k, "simt") == 0;
@@ -134,8 +135,8 @@ void Engine::launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, u
 void Engine::launch_crt_any(const uint32_t* d_y, uint32_t* d_c, uint32_t n0, uint32_t n1, cudaStream_t st) {
     if (simt_ || !crt_uses_tc(plan_)) {
         launch_crt(dp_, d_y, d_c, n0, n1, st);
-    } else if (crt_pipe_supported(dp_, d_y, n0, n1)) {
-        launch_crt_pipe(dp_, d_y, d_c, n0, n1, sms_, st);
+    } else if (crt_consts_ && crt_pipe_supported(dp_, d_y, n0, n1)) {
+        launch_crt_pipe(dp_, *crt_consts_, d_y, d_c, n0, n1, sms_, st);
     } else {
         launch_crt_tc(dp_, d_y, d_c, n0, n1, st);
     }

@@ -14,6 +14,8 @@
 
 namespace fpm {
 
+struct CrtConsts;
+
 class Engine {
 public:
     // Builds the plan and uploads it (throws std::runtime_error).
@@ -93,6 +95,7 @@ private:
     std::vector<cudaEvent_t> events_;
     std::vector<uint32_t> chunk_at_;  // I/O chunk boundaries (coefficients)
     std::unique_ptr<CopyPool> pool_;
+    std::shared_ptr<const CrtConsts> crt_consts_;   // pipelined CRT's kernel parameters
 };
 
 // Shared-memory opt-ins, once per device per process.

@@ -62,11 +62,19 @@ void launch_crt_tc(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n
                    cudaStream_t st);
 
 // The persistent CRT pipeline (crt_pipe.cu): one CTA per SM, `sms` at most.
-// Needs L >= 2 and N, n_begin, n_end multiples of 4.
+// Needs L >= 2 and N, n_begin, n_end multiples of 4.  Its per-prime constants
+// travel as a kernel parameter.
+struct CrtConsts {
+    uint32_t r50[kMaxK];        // floor(2^50 / p_j), for the rounding sum
+    uint32_t mlo[kMaxK + 1];    // top limb of constant j (j = K: -P mod q), low 16 bits
+    uint32_t mhi[kMaxK + 1];    // and high 16 bits
+    uint32_t q[kMaxL + 2];      // q, zero above L
+};
+CrtConsts make_crt_consts(const HostPlan& pl);
 bool crt_pipe_supported(const DevPoint& d, const uint32_t* Y, uint32_t n_begin, uint32_t n_end);
 void crt_pipe_init_attributes();
-void launch_crt_pipe(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n_begin, uint32_t n_end, int sms,
-                     cudaStream_t st);
+void launch_crt_pipe(const DevPoint& d, const CrtConsts& cc, const uint32_t* Y, uint32_t* c, uint32_t n_begin,
+                     uint32_t n_end, int sms, cudaStream_t st);
 
 // Grouped launches (group.cuh): one launch covers every item of the table,
 // whose first[] the caller fills with these per-item block counts.
