@@ -16,12 +16,12 @@
 // Organisation on the B200:
 //   * one CTA per SM walks super-tiles of 256 coefficients; TMEM's 512 columns
 //     hold the two 128-row halves of a super-tile (U <= 256 columns each);
-//   * warp 0 (one thread) streams y in with bulk copies (one 1 KB row per
-//     prime: y_j of the super-tile's 256 coefficients) and the constant image
-//     chunk by chunk, each through a two-slot ring;
-//   * warps 2-9, one thread per row, transpose y into the MMA's K-major byte
-//     layout, add up the rounding sum and the top limb, and put v in the last
-//     chunk;
+//   * warp 0 (one thread) streams the constant image in, chunk by chunk,
+//     through a two-slot ring;
+//   * warps 2-9, one thread per row, load y straight from HBM (coalesced,
+//     the next chunk's loads in flight under the current chunk's work), write
+//     it into the MMA's K-major byte layout, add up the rounding sum and the
+//     top limb, and put v in the last chunk;
 //   * warp 1 (one thread) issues the MMAs, two halves per chunk;
 //   * warps 10-17, one thread per row: a quotient estimate e from the top
 //     TMEM columns (within one of floor(X / q)), then one pass from the bottom
@@ -30,7 +30,7 @@
 //     the rare row that does not (about 2^-11 of them) adds or subtracts q in
 //     a second pass over what it stored.
 // Per-prime constants and q come from kernel parameters (constant bank), so
-// shared memory carries only y, the MMA operands and the per-row top limbs.
+// shared memory carries only the MMA operands and the per-row top limbs.
 // The kernel is compiled for the common limb counts (L = 64, 55, 28, 8) and
 // once for any L.
 //
@@ -51,16 +51,14 @@ constexpr int kEpiWarp0 = 10;             // warps 10-17
 constexpr uint32_t kSuper = 256;          // coefficients per super-tile
 constexpr uint32_t kChunk = 32;           // K rows (primes) per chunk
 constexpr int kMaxChunks = kMaxK / kChunk;   // K + 1 <= kMaxK rows
-constexpr uint32_t kSlot = 32768;         // bytes: y slot, A slot (two halves), B slot (U <= 256)
+constexpr uint32_t kSlot = 32768;         // bytes: A slot (two halves), B slot (U <= 256)
 constexpr int kX = kMaxL + 2;
 
 struct Smem {
-    uint8_t* yraw;       // [2][32 primes][256 coefficients] u32
     uint8_t* a;          // [2][2 halves][16 KB]
     uint8_t* b;          // [2][U x 128]
     uint4* meta;         // [2][256] {top limb words 0, 1, 2, -}
-    uint64_t* y_full;    // [2]
-    uint64_t* y_empty;   // [2]
+    uint32_t* outs;      // [2 halves][128 rows][out_stride(L)] result limbs
     uint64_t* b_full;    // [2]
     uint64_t* a_full;    // [2]
     uint64_t* mma_done;  // [2]
@@ -68,33 +66,49 @@ struct Smem {
     uint64_t* d_empty;   // [2]
     uint64_t* m_full;    // [2]
     uint64_t* m_empty;   // [2]
+    uint64_t* o_ready;   // [2] a half's result rows are in outs
+    uint64_t* o_free;    // [2] a half's rows have been copied out
     uint32_t* tmem_base;
     volatile uint32_t* abort;
 };
 
-constexpr size_t kMetaOff = 6 * size_t(kSlot);
-constexpr size_t kBarOff = kMetaOff + 2 * kSuper * sizeof(uint4);
+// Words per staged result row: a 16-byte-chunk stride that is odd (vector
+// rows, L a multiple of 4) or an odd word stride (scalar rows), so the
+// epilogue's row writes and the copy-out's reads are free of bank conflicts.
+__host__ __device__ constexpr int out_stride(int L) { return (L & 3) == 0 ? 4 * ((L / 4) | 1) : (L | 1); }
+constexpr int kMaxOutStride = out_stride(kMaxL);
+
+constexpr size_t kMetaOff = 4 * size_t(kSlot);
+constexpr size_t kOutOff = kMetaOff + 2 * kSuper * sizeof(uint4);
+constexpr size_t kBarOff = kOutOff + size_t(kSuper) * kMaxOutStride * 4;
 constexpr size_t kSmemBytes = kBarOff + 17 * 8 + 16;
 
 __device__ inline Smem carve(uint8_t* base) {
     Smem s;
-    s.yraw = base;
-    s.a = base + 2 * kSlot;
-    s.b = base + 4 * kSlot;
+    s.a = base;
+    s.b = base + 2 * kSlot;
     s.meta = reinterpret_cast<uint4*>(base + kMetaOff);
+    s.outs = reinterpret_cast<uint32_t*>(base + kOutOff);
     uint64_t* bars = reinterpret_cast<uint64_t*>(base + kBarOff);
-    s.y_full = bars;
-    s.y_empty = bars + 2;
-    s.b_full = bars + 4;
-    s.a_full = bars + 6;
-    s.mma_done = bars + 8;
-    s.d_full = bars + 10;
-    s.d_empty = bars + 11;
-    s.m_full = bars + 13;
-    s.m_empty = bars + 15;
+    s.b_full = bars;
+    s.a_full = bars + 2;
+    s.mma_done = bars + 4;
+    s.d_full = bars + 6;
+    s.d_empty = bars + 7;
+    s.m_full = bars + 9;
+    s.m_empty = bars + 11;
+    s.o_ready = bars + 13;
+    s.o_free = bars + 15;
     s.tmem_base = reinterpret_cast<uint32_t*>(bars + 17);
     s.abort = s.tmem_base + 1;
     return s;
+}
+
+// y_j of one coefficient, streamed past L1.
+__device__ __forceinline__ uint32_t ld_stream(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
 }
 
 // Bounded wait that also gives up once another role has raised the abort flag.
@@ -139,14 +153,14 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < 2; ++i) {
-            tc::mbar_init(&sm.y_full[i], 1);
-            tc::mbar_init(&sm.y_empty[i], 256);
             tc::mbar_init(&sm.b_full[i], 1);
             tc::mbar_init(&sm.a_full[i], 256);
             tc::mbar_init(&sm.mma_done[i], 1);
             tc::mbar_init(&sm.d_empty[i], 128);
             tc::mbar_init(&sm.m_full[i], 256);
             tc::mbar_init(&sm.m_empty[i], 256);
+            tc::mbar_init(&sm.o_ready[i], 128);
+            tc::mbar_init(&sm.o_free[i], 128);
         }
         tc::mbar_init(sm.d_full, 1);
         *sm.abort = 0;
@@ -159,25 +173,15 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t tmem = *sm.tmem_base;
 
     if (warp == 0) {
-        // ---- producer: y rows and constant chunks, two-slot rings ----
+        // ---- producer: constant chunks, two-slot ring ----
         if (lane == 0) {
             const uint32_t bbytes = U * 128;
-            uint32_t y_par[2] = {0, 0}, b_par[2] = {0, 0};   // parity of each slot's last arming
-            bool armed_y[2] = {false, false}, armed_b[2] = {false, false};
+            uint32_t b_par[2] = {0, 0};   // parity of each slot's last arming
+            bool armed_b[2] = {false, false};
             uint32_t g = 0;
             for (uint32_t t = blockIdx.x; t < tiles && !*sm.abort; t += gridDim.x) {
-                const uint32_t n0 = n_begin + t * kSuper;
-                const uint32_t rows = min(kSuper, n_end - n0);
                 for (int c = 0; c < nch; ++c, ++g) {
                     const int s = g & 1;
-                    if (g >= 2 && !wait_or_abort(&sm.y_empty[s], ((g - 2) >> 1) & 1, sm.abort)) break;
-                    const int j0 = c * kChunk, nj = max(0, min(static_cast<int>(kChunk), K - j0));
-                    tc::mbar_arrive_expect_tx(&sm.y_full[s], nj * rows * 4);
-                    for (int jj = 0; jj < nj; ++jj)
-                        tc::bulk_g2s(sm.yraw + s * kSlot + jj * kSuper * 4, Y + static_cast<size_t>(j0 + jj) * N + n0,
-                                     rows * 4, &sm.y_full[s]);
-                    y_par[s] = (g >> 1) & 1;
-                    armed_y[s] = true;
                     if (g >= 2 && !wait_or_abort(&sm.mma_done[s], ((g - 2) >> 1) & 1, sm.abort)) break;
                     tc::mbar_arrive_expect_tx(&sm.b_full[s], bbytes);
                     tc::bulk_g2s(sm.b + s * kSlot, d.crt_img_v + static_cast<size_t>(c) * bbytes, bbytes,
@@ -189,7 +193,6 @@ __global__ void __launch_bounds__(kThreads, 1)
             }
             // Copies still in flight must land before the CTA may exit.
             for (int s = 0; s < 2; ++s) {
-                if (armed_y[s]) tc::wait_parity(&sm.y_full[s], y_par[s]);
                 if (armed_b[s]) tc::wait_parity(&sm.b_full[s], b_par[s]);
             }
         }
@@ -244,21 +247,30 @@ __global__ void __launch_bounds__(kThreads, 1)
         for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
             const uint32_t n0 = n_begin + t * kSuper;
             const bool live = row < min(kSuper, n_end - n0);
+            const uint32_t* yrow = Y + n0 + row;
             uint64_t vacc = 0, tlo = 0, thi = 0;   // sum y r50; sum y (top & 0xFFFF); sum y (top >> 16)
             bool ok = true;
+            uint32_t ya[kChunk], yb[kChunk];
+#pragma unroll
+            for (int jj = 0; jj < static_cast<int>(kChunk); ++jj)
+                ya[jj] = (live && jj < K) ? ld_stream(yrow + static_cast<size_t>(jj) * N) : 0u;
 #pragma unroll
             for (int c = 0; c < kMaxChunks; ++c) {
                 if (c >= nch) break;
+                uint32_t(&yv)[kChunk] = (c & 1) ? yb : ya;
+                uint32_t(&yn)[kChunk] = (c & 1) ? ya : yb;
+                if (c + 1 < kMaxChunks && c + 1 < nch) {
+                    // The next chunk's loads go out before this chunk's work.
+#pragma unroll
+                    for (int jj = 0; jj < static_cast<int>(kChunk); ++jj) {
+                        const int j = (c + 1) * static_cast<int>(kChunk) + jj;
+                        yn[jj] = (live && j < K) ? ld_stream(yrow + static_cast<size_t>(j) * N) : 0u;
+                    }
+                }
                 const int s = g & 1;
-                ok = wait_or_abort(&sm.y_full[s], (g >> 1) & 1, sm.abort);
-                if (ok && g >= 2) ok = wait_or_abort(&sm.mma_done[s], ((g - 2) >> 1) & 1, sm.abort);
+                if (g >= 2) ok = wait_or_abort(&sm.mma_done[s], ((g - 2) >> 1) & 1, sm.abort);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
-                const uint32_t* ys = reinterpret_cast<const uint32_t*>(sm.yraw + s * kSlot);
-                uint32_t yv[kChunk];
-#pragma unroll
-                for (int jj = 0; jj < static_cast<int>(kChunk); ++jj)
-                    yv[jj] = (live && c * static_cast<int>(kChunk) + jj < K) ? ys[jj * kSuper + row] : 0u;
 #pragma unroll
                 for (int jj = 0; jj < static_cast<int>(kChunk); ++jj) {
                     const int j = c * static_cast<int>(kChunk) + jj;
@@ -286,7 +298,6 @@ __global__ void __launch_bounds__(kThreads, 1)
                         make_uint4(yv[4 * q4], yv[4 * q4 + 1], yv[4 * q4 + 2], yv[4 * q4 + 3]);
                 tc::fence_proxy_async_smem();
                 tc::mbar_arrive(&sm.a_full[s]);
-                tc::mbar_arrive(&sm.y_empty[s]);
                 ++g;
             }
             if (!ok) break;
@@ -312,7 +323,11 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t npieces = U / 16;
         const int n = L + 2, drop = top_drop(L);
         const uint32_t top_piece = static_cast<uint32_t>(4 * drop) / 16;
-        const bool vec = (L & 3) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+        const bool svec = (L & 3) == 0;                                             // 16-byte rows in outs
+        const bool gvec = svec && (reinterpret_cast<uintptr_t>(C) & 15) == 0;      // 16-byte global stores
+        const int ostride = LT > 0 ? out_stride(LT) : out_stride(L);
+        const uint32_t hrow = qd * 32 + lane;                                       // row within the half
+        uint32_t* srow = sm.outs + (h * 128 + hrow) * ostride;
         constexpr int kXL = LT > 0 ? LT + 2 : kX;        // limbs handled
         constexpr int kPieces = (kXL + 3) / 4;
         uint32_t it = 0;
@@ -346,7 +361,12 @@ __global__ void __launch_bounds__(kThreads, 1)
             const double f = floor(xd * d.q_top_inv);
             const uint64_t e = f > 0 ? static_cast<uint64_t>(f) : 0;
             const uint32_t e_lo = static_cast<uint32_t>(e), e_hi = static_cast<uint32_t>(e >> 32);
-            uint32_t* out = C + static_cast<size_t>(n0 + row) * L;
+            if (it >= 1) {
+                // The previous super-tile's rows of this half have left outs.
+                ok = wait_or_abort(&sm.o_free[h], (it - 1) & 1, sm.abort);
+                ok = __all_sync(0xffffffffu, ok);
+                if (!ok) break;
+            }
             // One pass from the bottom: X with carries, minus e q; the borrows
             // of X - e q (b0) and of (X - e q) - q (b1).  TMEM pieces are
             // double-buffered: piece pc + 1 loads while piece pc is used.
@@ -386,11 +406,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                         b0 = static_cast<uint32_t>(dy >> 63);
                         b1 = static_cast<uint32_t>((static_cast<uint64_t>(yk) - qk - b1) >> 63);
                         o[i] = yk;
-                        if (k < L && live) {
-                            if (vec) {
-                                if (i == 3) *reinterpret_cast<uint4*>(out + k - 3) = make_uint4(o[0], o[1], o[2], o[3]);
+                        if (k < L) {
+                            if (svec) {
+                                if (i == 3) *reinterpret_cast<uint4*>(srow + k - 3) = make_uint4(o[0], o[1], o[2], o[3]);
                             } else {
-                                out[k] = yk;
+                                srow[k] = yk;
                             }
                         }
                     }
@@ -404,18 +424,44 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (live && (b0 || !b1)) {
                 uint32_t cb = 0;
                 for (int k = 0; k < L; ++k) {
-                    const uint32_t x = out[k], qk = cc.q[k];
+                    const uint32_t x = srow[k], qk = cc.q[k];
                     if (b0) {
                         const uint64_t sum = static_cast<uint64_t>(x) + qk + cb;
-                        out[k] = static_cast<uint32_t>(sum);
+                        srow[k] = static_cast<uint32_t>(sum);
                         cb = static_cast<uint32_t>(sum >> 32);
                     } else {
                         const uint64_t dd = static_cast<uint64_t>(x) - qk - cb;
-                        out[k] = static_cast<uint32_t>(dd);
+                        srow[k] = static_cast<uint32_t>(dd);
                         cb = static_cast<uint32_t>(dd >> 63);
                     }
                 }
             }
+            // The half's 128 rows are one contiguous run of c: copy it out
+            // with coalesced stores once every row is in outs.
+            tc::mbar_arrive(&sm.o_ready[h]);
+            ok = wait_or_abort(&sm.o_ready[h], it & 1, sm.abort);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) break;
+            {
+                const int rows_h = max(0, min(128, static_cast<int>(min(kSuper, n_end - n0)) - static_cast<int>(128 * h)));
+                uint32_t* gbase = C + static_cast<size_t>(n0 + 128 * h) * L;
+                const uint32_t* sbase = sm.outs + h * 128 * ostride;
+                if (gvec) {
+                    const int q4 = L / 4, n4 = rows_h * q4;
+                    for (int i4 = static_cast<int>(hrow); i4 < n4; i4 += 128) {
+                        const int r = i4 / q4, c4 = i4 - r * q4;
+                        *reinterpret_cast<uint4*>(gbase + 4 * i4) =
+                            *reinterpret_cast<const uint4*>(sbase + r * ostride + 4 * c4);
+                    }
+                } else {
+                    const int nw = rows_h * L;
+                    for (int i = static_cast<int>(hrow); i < nw; i += 128) {
+                        const int r = i / L;
+                        gbase[i] = sbase[r * ostride + (i - r * L)];
+                    }
+                }
+            }
+            tc::mbar_arrive(&sm.o_free[h]);
         }
     }
 
