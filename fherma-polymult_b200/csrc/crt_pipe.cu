@@ -39,6 +39,7 @@
 // and the error word gets bit 1.
 #include "device.cuh"
 #include "kernels.h"
+#include "pdl.cuh"
 #include "tc.cuh"
 
 namespace fpm {
@@ -142,6 +143,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     k_crt_pipe(DevPoint d, const __grid_constant__ CrtConsts cc, const uint32_t* __restrict__ Y,
                uint32_t* __restrict__ C, uint32_t n_begin, uint32_t n_end) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
+    pdl_launch_dependents();
     const Smem sm = carve(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int L = LT > 0 ? LT : d.L;
@@ -171,6 +173,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *sm.tmem_base;
+    pdl_wait();   // y and c belong to the kernels around this one
 
     if (warp == 0) {
         // ---- producer: constant chunks, two-slot ring ----
@@ -516,13 +519,15 @@ void launch_crt_pipe(const DevPoint& d, const CrtConsts& cc, const uint32_t* Y, 
     if (n_end <= n_begin) return;
     const uint32_t tiles = (n_end - n_begin + kSuper - 1) / kSuper;
     const uint32_t grid = tiles < static_cast<uint32_t>(sms) ? tiles : static_cast<uint32_t>(sms);
+    cudaError_t e = cudaSuccess;
     switch (d.L) {
-        case 64: k_crt_pipe<64><<<grid, kThreads, kSmemBytes, st>>>(d, cc, Y, c, n_begin, n_end); break;
-        case 55: k_crt_pipe<55><<<grid, kThreads, kSmemBytes, st>>>(d, cc, Y, c, n_begin, n_end); break;
-        case 28: k_crt_pipe<28><<<grid, kThreads, kSmemBytes, st>>>(d, cc, Y, c, n_begin, n_end); break;
-        case 8: k_crt_pipe<8><<<grid, kThreads, kSmemBytes, st>>>(d, cc, Y, c, n_begin, n_end); break;
-        default: k_crt_pipe<0><<<grid, kThreads, kSmemBytes, st>>>(d, cc, Y, c, n_begin, n_end); break;
+        case 64: e = launch_pdl(k_crt_pipe<64>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, Y, c, n_begin, n_end); break;
+        case 55: e = launch_pdl(k_crt_pipe<55>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, Y, c, n_begin, n_end); break;
+        case 28: e = launch_pdl(k_crt_pipe<28>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, Y, c, n_begin, n_end); break;
+        case 8: e = launch_pdl(k_crt_pipe<8>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, Y, c, n_begin, n_end); break;
+        default: e = launch_pdl(k_crt_pipe<0>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, Y, c, n_begin, n_end); break;
     }
+    check(e, "crt launch");
 }
 
 }  // namespace fpm

@@ -25,6 +25,7 @@
 #include "device.cuh"
 #include "group.cuh"
 #include "kernels.h"
+#include "pdl.cuh"
 #include "tc.cuh"
 
 namespace fpm {
@@ -98,6 +99,9 @@ __device__ __forceinline__ void dec_body(const DevPoint& d, const uint32_t* __re
     if (warp == 0) tc::tmem_alloc(sm.tmem_base, 2 * kCols);
     for (int j = threadIdx.x; j < d.K; j += kThreads) sm.fold[j] = d.dec_fold[j];
 
+    // The operand tile and the residues are the only global data a preceding
+    // kernel may still be using.
+    pdl_wait();
     // Operand tile: word l of row m goes to core matrix l / 4 along K, row m.
     // The block's nk L words are contiguous and 16-byte aligned (n0 L 4 = 512 L
     // bytes), so they are read as 16-byte chunks, 8 in flight per thread.
@@ -241,6 +245,7 @@ __global__ void __launch_bounds__(kThreads)
     k_decompose_tc(DevPoint d, const uint32_t* __restrict__ la, const uint32_t* __restrict__ lb,
                    uint32_t* __restrict__ ra, uint32_t* __restrict__ rb, int operand0, uint32_t n_begin,
                    uint32_t n_end) {
+    pdl_launch_dependents();
     const uint32_t n0 = n_begin + blockIdx.x * kRows;
     const bool second = blockIdx.y != 0;
     dec_body(d, second ? lb : la, second ? rb : ra, operand0 + static_cast<int>(blockIdx.y), n0,
@@ -286,14 +291,16 @@ void launch_decompose_tc(const DevPoint& d, const uint32_t* limbs, uint32_t* res
                          uint32_t n_end, cudaStream_t st) {
     if (n_end <= n_begin) return;
     const uint32_t blocks = (n_end - n_begin + kRows - 1) / kRows;
-    k_decompose_tc<<<blocks, kThreads, smem_bytes(d.dec_kb), st>>>(d, limbs, limbs, res, res, operand, n_begin,
-                                                                    n_end);
+    check(launch_pdl(k_decompose_tc, dim3(blocks), dim3(kThreads), smem_bytes(d.dec_kb), st, d, limbs, limbs, res,
+                     res, operand, n_begin, n_end),
+          "decompose launch");
 }
 
 void launch_decompose_tc_pair(const DevPoint& d, const uint32_t* a, const uint32_t* b, uint32_t* A, uint32_t* B,
                               cudaStream_t st) {
     const dim3 grid((d.N + kRows - 1) / kRows, 2);
-    k_decompose_tc<<<grid, kThreads, smem_bytes(d.dec_kb), st>>>(d, a, b, A, B, 0, 0, d.N);
+    check(launch_pdl(k_decompose_tc, grid, dim3(kThreads), smem_bytes(d.dec_kb), st, d, a, b, A, B, 0, 0u, d.N),
+          "decompose launch");
 }
 
 }  // namespace fpm

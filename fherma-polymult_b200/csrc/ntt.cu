@@ -21,6 +21,7 @@
 #include "group.cuh"
 #include "kernels.h"
 #include "ntt_engine.cuh"
+#include "pdl.cuh"
 
 #include <type_traits>
 
@@ -353,16 +354,22 @@ __host__ __device__ __forceinline__ uint32_t row_blocks(uint32_t logR) {
 // Plain launches: grid (blocks per prime, K).
 template <int LOGR, bool LAZY>
 __global__ void __launch_bounds__(kNttThreads) k_ntt_col_fwd(DevPoint d, uint32_t* A, uint32_t* B) {
+    pdl_launch_dependents();
+    pdl_wait();
     col_fwd_body<LOGR, LAZY>(d, A, B, blockIdx.y, blockIdx.x);
 }
 
 template <int LOGR, bool LAZY>
 __global__ void __launch_bounds__(kNttThreads) k_ntt_col_inv(DevPoint d, uint32_t* A) {
+    pdl_launch_dependents();
+    pdl_wait();
     col_inv_body<LOGR, LAZY>(d, A, blockIdx.y, blockIdx.x);
 }
 
 template <int LOGS, bool LAZY>
 __global__ void __launch_bounds__(kNttThreads, 5) k_ntt_row(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
+    pdl_launch_dependents();
+    pdl_wait();
     row_body<LOGS, LAZY>(d, A, B, mode, blockIdx.y, blockIdx.x);
 }
 
@@ -537,13 +544,15 @@ void attrs_all() {
 template <int LOGR, bool LAZY>
 void launch_col_fwd_t(const DevPoint& d, uint32_t* A, uint32_t* B, cudaStream_t st) {
     const dim3 grid((1u << d.logS) >> (11 - LOGR), d.K);
-    k_ntt_col_fwd<LOGR, LAZY><<<grid, kNttThreads, col_fwd_smem_t(LOGR), st>>>(d, A, B);
+    check(launch_pdl(k_ntt_col_fwd<LOGR, LAZY>, grid, dim3(kNttThreads), col_fwd_smem_t(LOGR), st, d, A, B),
+          "col_fwd launch");
 }
 
 template <int LOGR, bool LAZY>
 void launch_col_inv_t(const DevPoint& d, uint32_t* A, cudaStream_t st) {
     const dim3 grid((1u << d.logS) >> (11 - LOGR), d.K);
-    k_ntt_col_inv<LOGR, LAZY><<<grid, kNttThreads, col_inv_smem_t(LOGR), st>>>(d, A);
+    check(launch_pdl(k_ntt_col_inv<LOGR, LAZY>, grid, dim3(kNttThreads), col_inv_smem_t(LOGR), st, d, A),
+          "col_inv launch");
 }
 
 template <int LOGS, bool LAZY>
@@ -551,7 +560,8 @@ void launch_row_t(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStr
     using RG = RowGeom<LOGS>;
     const uint32_t R = 1u << d.logR;
     const dim3 grid(RG::G >= 2 ? R / RG::G : R, d.K);
-    k_ntt_row<LOGS, LAZY><<<grid, kNttThreads, row_smem_t<LOGS>(), st>>>(d, A, B, mode);
+    check(launch_pdl(k_ntt_row<LOGS, LAZY>, grid, dim3(kNttThreads), row_smem_t<LOGS>(), st, d, A, B, mode),
+          "row launch");
 }
 
 template <bool LAZY>
