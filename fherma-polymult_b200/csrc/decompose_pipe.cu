@@ -1,0 +1,306 @@
+// Decompose on the tensor cores as a persistent, warp-specialised pipeline.
+//
+// Same arithmetic as decompose_tc.cu (reference decompose_many rns.cuh:110-128):
+//
+//     D[m][4j + s] = sum_k byte_k(x_m) * byte_s(2^(8k) sigma_j mod p_j)   (< 2^24)
+//     x_m mod p_j  = (sum_s D[m][4j + s] 2^(8s)) mod p_j
+//
+// Organisation on the B200: one CTA per SM works on one operand (a pair launch
+// splits the CTAs between a and b) and walks its 128-coefficient tiles:
+//   * warp 0 loads the operand's whole constant image once (up to 5 chunks of
+//     32 primes x 4 bytes x 4L bytes: 160 KB, resident in shared memory) and
+//     then, one thread, issues the MMAs: per chunk D goes to one of four
+//     128-column TMEM buffers;
+//   * warps 1-4 stage the next tile's limbs into a two-slot ring in the MMA's
+//     K-major layout (coalesced 16-byte loads, conflict-free stores thanks to a
+//     padded K stride) while the current tile is multiplied and folded;
+//   * warps 5-20, four per TMEM lane quadrant, one coefficient per thread,
+//     each take 8 of a chunk's 32 primes: read D, fold the 49-bit sums mod p_j
+//     and store the residues (a warp writes 32 consecutive words per prime).
+// The fold constants come from kernel parameters.  Every wait is bounded; a
+// timeout raises an abort flag that every role checks, and the error word gets
+// bit 0.
+#include "device.cuh"
+#include "kernels.h"
+#include "pdl.cuh"
+#include "tc.cuh"
+
+namespace fpm {
+
+namespace {
+
+constexpr int kThreads = 672;                      // 21 warps
+constexpr int kLoadWarp0 = 1;                      // warps 1-4
+constexpr int kLoaders = 128;
+constexpr int kEpiWarp0 = 5;                       // warps 5-20
+constexpr int kEpi = 512;
+constexpr uint32_t kRows = 128;
+constexpr uint32_t kCols = 128;                    // GEMM columns per chunk (32 primes)
+constexpr uint32_t kALbo = kRows * 16 + 16;        // K stride of the operand tile, padded
+
+__host__ __device__ inline uint32_t a_bytes(uint32_t kb) { return (kb / 16) * kALbo; }
+__host__ __device__ inline size_t b_bytes(uint32_t kb, int nch) { return static_cast<size_t>(nch) * kCols * kb; }
+__host__ inline size_t smem_bytes(uint32_t kb, int nch) { return b_bytes(kb, nch) + 2 * a_bytes(kb) + 128; }
+
+struct Smem {
+    uint8_t* b;            // resident constant image
+    uint8_t* a;            // [2] operand tiles
+    uint64_t* b_full;      // [1]
+    uint64_t* a_full;      // [2]
+    uint64_t* a_empty;     // [2]
+    uint64_t* d_full;      // [4]
+    uint64_t* d_empty;     // [4]
+    uint32_t* tmem_base;
+    volatile uint32_t* abort;
+};
+
+__device__ inline Smem carve(uint8_t* base, uint32_t kb, int nch) {
+    Smem s;
+    s.b = base;
+    s.a = base + b_bytes(kb, nch);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(s.a + 2 * a_bytes(kb));
+    s.b_full = bars;
+    s.a_full = bars + 1;
+    s.a_empty = bars + 3;
+    s.d_full = bars + 5;
+    s.d_empty = bars + 9;
+    s.tmem_base = reinterpret_cast<uint32_t*>(bars + 13);
+    s.abort = s.tmem_base + 1;
+    return s;
+}
+
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile uint32_t* abort) {
+    if (tc::mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = tc::globaltimer();
+    while (!tc::mbar_try_wait(bar, parity)) {
+        if (*abort) return false;
+        if (tc::globaltimer() - t0 > tc::kWaitNs) {
+            *abort = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+// (lo + hi 2^32) mod p for the 49-bit sums: f = {p, 2^32 mod p, its Shoup
+// companion, floor(2^32 / p)}.
+__device__ __forceinline__ uint32_t fold49(uint64_t v, uint4 f) {
+    const uint32_t lo = shoup(static_cast<uint32_t>(v), 1u, f.w, f.x);
+    const uint32_t hi = shoup(static_cast<uint32_t>(v >> 32), f.y, f.z, f.x);
+    return add_mod(lo, hi, f.x);
+}
+
+// CTAs [0, split) take operand 0 (la -> ra), [split, gridDim.x) operand 1.
+__global__ void __launch_bounds__(kThreads, 1)
+    k_decompose_pipe(DevPoint d, const __grid_constant__ DecConsts fc, const uint32_t* __restrict__ la,
+                     const uint32_t* __restrict__ lb, uint32_t* __restrict__ ra, uint32_t* __restrict__ rb,
+                     int operand0, uint32_t n_begin, uint32_t n_end, uint32_t split) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    pdl_launch_dependents();
+    const uint32_t kb = d.dec_kb;
+    const int nch = d.dec_chunks;
+    const Smem sm = carve(smem_raw, kb, nch);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int L = d.L, K = d.K;
+    const bool second = blockIdx.x >= split;
+    const int operand = operand0 + (second ? 1 : 0);
+    const uint32_t* limbs = second ? lb : la;
+    uint32_t* res = second ? rb : ra;
+    const uint8_t* img = operand ? d.dec_img_b : d.dec_img_a;
+    const uint32_t g0 = second ? split : 0, gs = second ? gridDim.x - split : split;
+    const uint32_t tiles = (n_end - n_begin + kRows - 1) / kRows;
+    const uint32_t chunk_bytes = kCols * kb;
+
+    if (threadIdx.x == 0) {
+        tc::mbar_init(sm.b_full, 1);
+        for (int i = 0; i < 2; ++i) {
+            tc::mbar_init(&sm.a_full[i], kLoaders);
+            tc::mbar_init(&sm.a_empty[i], 1);
+        }
+        for (int i = 0; i < 4; ++i) {
+            tc::mbar_init(&sm.d_full[i], 1);
+            tc::mbar_init(&sm.d_empty[i], kEpi);
+        }
+        *sm.abort = 0;
+        tc::fence_mbar_init();
+        // The constant image is read-only plan data: it loads under the
+        // preceding kernel's tail.
+        tc::mbar_arrive_expect_tx(sm.b_full, static_cast<uint32_t>(b_bytes(kb, nch)));
+        for (int c = 0; c < nch; ++c)
+            tc::bulk_g2s(sm.b + c * chunk_bytes, img + static_cast<size_t>(c) * chunk_bytes, chunk_bytes, sm.b_full);
+    }
+    if (warp == 0) tc::tmem_alloc(sm.tmem_base, 512);
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = *sm.tmem_base;
+    pdl_wait();   // the limbs and the residues belong to the kernels around this one
+
+    if (warp == 0) {
+        // ---- MMA issuer ----
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_u8(kCols);
+            bool ok = wait_or_abort(sm.b_full, 0, sm.abort);
+            uint64_t* last_bar = nullptr;   // the barrier of the latest commit
+            uint32_t last_par = 0;
+            uint32_t g = 0, i = 0;
+            for (uint32_t t = blockIdx.x - g0; ok && t < tiles; t += gs, ++i) {
+                const int s = i & 1;
+                ok = wait_or_abort(&sm.a_full[s], (i >> 1) & 1, sm.abort);
+                if (!ok) break;
+                const uint32_t a0 = tc::smem_addr(sm.a + s * a_bytes(kb));
+                for (int c = 0; c < nch; ++c, ++g) {
+                    const int buf = g & 3;
+                    if (g >= 4) {
+                        ok = wait_or_abort(&sm.d_empty[buf], ((g - 4) >> 2) & 1, sm.abort);
+                        if (!ok) break;
+                    }
+                    tc::tc_fence_after();
+                    const uint32_t b0 = tc::smem_addr(sm.b + c * chunk_bytes);
+                    for (uint32_t kk = 0; kk < kb / 32; ++kk) {
+                        const uint64_t ad = tc::smem_desc(a0 + kk * 2 * kALbo, kALbo, 128);
+                        const uint64_t bd = tc::smem_desc(b0 + kk * 2 * (kCols * 16), kCols * 16, 128);
+                        tc::mma_u8(tmem + buf * kCols, ad, bd, idesc, kk > 0);
+                    }
+                    tc::mma_commit(&sm.d_full[buf]);
+                    last_bar = &sm.d_full[buf];
+                    last_par = (g >> 2) & 1;
+                }
+                if (!ok) break;
+                tc::mma_commit(&sm.a_empty[s]);
+                last_bar = &sm.a_empty[s];
+                last_par = (i >> 1) & 1;
+            }
+            // MMAs still running must finish before the CTA may exit.
+            if (last_bar) tc::wait_parity(last_bar, last_par);
+        }
+        __syncwarp();
+    } else if (warp < kEpiWarp0) {
+        // ---- loaders: the next tile's limbs, K-major with a padded K stride ----
+        const uint32_t lt = threadIdx.x - kLoadWarp0 * 32;
+        const bool vec = (reinterpret_cast<uintptr_t>(limbs) & 15u) == 0 && (L & 3) == 0;
+        const uint32_t kw = kb / 4;
+        uint32_t i = 0;
+        for (uint32_t t = blockIdx.x - g0; t < tiles; t += gs, ++i) {
+            const int s = i & 1;
+            if (i >= 2) {
+                bool ok = wait_or_abort(&sm.a_empty[s], ((i - 2) >> 1) & 1, sm.abort);
+                ok = __all_sync(0xffffffffu, ok);
+                if (!ok) break;
+            }
+            uint8_t* at = sm.a + s * a_bytes(kb);
+            const uint32_t n0 = n_begin + t * kRows;
+            const uint32_t nk = min(kRows, n_end - n0);
+            // Every position of the tile is written once: a limb, or zero for
+            // rows past nk and limbs past L.
+            if (vec) {
+                // 16-byte group gq of row m is limbs 4 gq .. 4 gq + 3.
+                const uint32_t q4 = static_cast<uint32_t>(L) / 4, G = kb / 16, n16 = kRows * G;
+                const uint4* src4 = reinterpret_cast<const uint4*>(limbs + static_cast<size_t>(n0) * L);
+                for (uint32_t w0 = lt; w0 < n16; w0 += 8 * kLoaders) {
+                    uint4 v[8];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const uint32_t w = w0 + k * kLoaders, mm = w / G, gq = w - mm * G;
+                        v[k] = (w < n16 && mm < nk && gq < q4) ? __ldg(src4 + mm * q4 + gq) : make_uint4(0, 0, 0, 0);
+                    }
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const uint32_t w = w0 + k * kLoaders, mm = w / G, gq = w - mm * G;
+                        if (w < n16) *reinterpret_cast<uint4*>(at + gq * kALbo + mm * 16) = v[k];
+                    }
+                }
+            } else {
+                const uint32_t* src = limbs + static_cast<size_t>(n0) * L;
+                for (uint32_t w = lt; w < kRows * kw; w += kLoaders) {
+                    const uint32_t mm = w / kw, l = w - mm * kw;
+                    const uint32_t v = (mm < nk && l < static_cast<uint32_t>(L)) ? src[mm * L + l] : 0u;
+                    *reinterpret_cast<uint32_t*>(at + (l >> 2) * kALbo + mm * 16 + (l & 3) * 4) = v;
+                }
+            }
+            tc::fence_proxy_async_smem();
+            tc::mbar_arrive(&sm.a_full[s]);
+        }
+    } else {
+        // ---- epilogue: thread = one coefficient, 8 primes of each chunk ----
+        const int ew = warp - kEpiWarp0;
+        const uint32_t qd = warp & 3, piece = ew >> 2;
+        const uint32_t m = qd * 32 + lane;
+        const uint32_t tq = tmem + ((qd * 32) << 16) + piece * 32;
+        uint32_t g = 0;
+        for (uint32_t t = blockIdx.x - g0; t < tiles; t += gs) {
+            const uint32_t n0 = n_begin + t * kRows;
+            const bool live = m < min(kRows, n_end - n0);
+            bool ok = true;
+            for (int c = 0; c < nch; ++c, ++g) {
+                const int buf = g & 3;
+                ok = wait_or_abort(&sm.d_full[buf], (g >> 2) & 1, sm.abort);
+                ok = __all_sync(0xffffffffu, ok);
+                if (!ok) break;
+                tc::tc_fence_after();
+                const int j0 = c * 32 + static_cast<int>(piece) * 8;
+                uint32_t r[32];
+                tc::tmem_ld32(tq + buf * kCols, r);
+                tc::tmem_ld_wait();
+                tc::tc_fence_before();
+                tc::mbar_arrive(&sm.d_empty[buf]);
+                if (j0 < K) {
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) {
+                        const int j = j0 + k;
+                        const uint64_t v = static_cast<uint64_t>(r[4 * k]) + (static_cast<uint64_t>(r[4 * k + 1]) << 8) +
+                                           (static_cast<uint64_t>(r[4 * k + 2]) << 16) +
+                                           (static_cast<uint64_t>(r[4 * k + 3]) << 24);
+                        if (live && j < K) res[static_cast<size_t>(j) * d.N + n0 + m] = fold49(v, fc.fold[j]);
+                    }
+                }
+            }
+            if (!ok) break;
+        }
+    }
+
+    tc::tc_fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0 && *sm.abort) atomicOr(d.err, 1u);
+    if (warp == 0) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, 512);
+    }
+}
+
+}  // namespace
+
+DecConsts make_dec_consts(const HostPlan& pl) {
+    DecConsts dc{};
+    for (int j = 0; j < pl.K; ++j) dc.fold[j] = pl.dec_fold[j];
+    return dc;
+}
+
+bool decompose_pipe_supported(const DevPoint& d) {
+    return d.dec_chunks >= 1 && d.dec_chunks <= static_cast<int>(kMaxK / 32) && d.K <= kMaxK &&
+           smem_bytes(d.dec_kb, d.dec_chunks) <= 227 * 1024;
+}
+
+void decompose_pipe_init_attributes() {
+    check(cudaFuncSetAttribute(k_decompose_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+          "decompose_pipe smem");
+}
+
+void launch_decompose_pipe(const DevPoint& d, const DecConsts& dc, const uint32_t* a, const uint32_t* b,
+                           uint32_t* A, uint32_t* B, int operand0, uint32_t n_begin, uint32_t n_end, int sms,
+                           cudaStream_t st) {
+    if (n_end <= n_begin) return;
+    const uint32_t tiles = (n_end - n_begin + kRows - 1) / kRows;
+    const int operands = b ? 2 : 1;
+    // CTAs per operand: one per SM in all, no more than the operand's tiles.
+    uint32_t per = static_cast<uint32_t>(sms) / operands;
+    if (per < 1) per = 1;
+    if (per > tiles) per = tiles;
+    const uint32_t grid = per * operands;
+    const uint32_t split = operands == 2 ? per : grid;
+    check(launch_pdl(k_decompose_pipe, dim3(grid), dim3(kThreads), smem_bytes(d.dec_kb, d.dec_chunks), st, d, dc, a,
+                     b ? b : a, A, B ? B : A, operand0, n_begin, n_end, split),
+          "decompose launch");
+}
+
+}  // namespace fpm

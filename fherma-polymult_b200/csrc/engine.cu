@@ -29,6 +29,7 @@ void ensure_kernel_attributes(int device) {
     decompose_tc_init_attributes();
     crt_tc_init_attributes();
     crt_pipe_init_attributes();
+    decompose_pipe_init_attributes();
     done.push_back(device);
 }
 
@@ -88,6 +89,7 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
         dp_.crt_img_v = upload(pl.crt_img_v);
         dp_.negp_top = pl.negp_top;
         if (crt_uses_tc(pl)) crt_consts_.reset(new CrtConsts(make_crt_consts(pl)));
+        if (decompose_pipe_supported(dp_)) dec_consts_.reset(new DecConsts(make_dec_consts(pl)));
         dp_.err = dalloc<uint32_t>(1);
         check(cudaMemset(dp_.err, 0, sizeof(uint32_t)), "memset");
         if (const char* k = std::getenv("FPM_KERNELS")) simt_ = std::strcmp(k, "simt") == 0;
@@ -127,6 +129,8 @@ void Engine::launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, u
                         cudaStream_t st) {
     if (simt_) {
         launch_decompose(dp_, d_limbs, d_res, operand, n0, n1, st);
+    } else if (dec_consts_) {
+        launch_decompose_pipe(dp_, *dec_consts_, d_limbs, nullptr, d_res, nullptr, operand, n0, n1, sms_, st);
     } else {
         launch_decompose_tc(dp_, d_limbs, d_res, operand, n0, n1, st);
     }
@@ -168,6 +172,8 @@ void Engine::run_device(const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,
     if (simt_) {
         launch_dec(d_a, A_, 0, 0, plan_.N, st);
         launch_dec(d_b, B_, 1, 0, plan_.N, st);
+    } else if (dec_consts_) {
+        launch_decompose_pipe(dp_, *dec_consts_, d_a, d_b, A_, B_, 0, 0, plan_.N, sms_, st);
     } else {
         launch_decompose_tc_pair(dp_, d_a, d_b, A_, B_, st);
     }

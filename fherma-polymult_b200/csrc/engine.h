@@ -15,6 +15,7 @@
 namespace fpm {
 
 struct CrtConsts;
+struct DecConsts;
 
 class Engine {
 public:
@@ -96,6 +97,7 @@ private:
     std::vector<uint32_t> chunk_at_;  // I/O chunk boundaries (coefficients)
     std::unique_ptr<CopyPool> pool_;
     std::shared_ptr<const CrtConsts> crt_consts_;   // pipelined CRT's kernel parameters
+    std::shared_ptr<const DecConsts> dec_consts_;   // pipelined decompose's kernel parameters
 };
 
 // Shared-memory opt-ins, once per device per process.

@@ -76,6 +76,19 @@ void crt_pipe_init_attributes();
 void launch_crt_pipe(const DevPoint& d, const CrtConsts& cc, const uint32_t* Y, uint32_t* c, uint32_t n_begin,
                      uint32_t n_end, int sms, cudaStream_t st);
 
+// The persistent decompose pipeline (decompose_pipe.cu): one CTA per SM; with
+// b != nullptr the CTAs split between a -> A (operand 0) and b -> B (1),
+// otherwise all take a -> A as operand `operand0`.
+struct DecConsts {
+    uint4 fold[kMaxK];          // {p, 2^32 mod p, its Shoup companion, floor(2^32 / p)}
+};
+DecConsts make_dec_consts(const HostPlan& pl);
+bool decompose_pipe_supported(const DevPoint& d);
+void decompose_pipe_init_attributes();
+void launch_decompose_pipe(const DevPoint& d, const DecConsts& dc, const uint32_t* a, const uint32_t* b,
+                           uint32_t* A, uint32_t* B, int operand0, uint32_t n_begin, uint32_t n_end, int sms,
+                           cudaStream_t st);
+
 // Grouped launches (group.cuh): one launch covers every item of the table,
 // whose first[] the caller fills with these per-item block counts.
 struct GroupTable;
