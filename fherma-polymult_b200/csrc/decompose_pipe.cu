@@ -7,16 +7,20 @@
 //
 // Organisation on the B200: one CTA per SM works on one operand (a pair launch
 // splits the CTAs between a and b) and walks its 128-coefficient tiles:
-//   * warp 0 loads the operand's whole constant image once (up to 5 chunks of
-//     32 primes x 4 bytes x 4L bytes: 160 KB, resident in shared memory) and
-//     then, one thread, issues the MMAs: per chunk D goes to one of four
-//     128-column TMEM buffers;
+//   * warp 0 loads the operand's whole constant image once (chunks of 64
+//     primes x 4 bytes x 4L bytes, the last one packed: at most 160 KB,
+//     resident in shared memory) and then, one thread, issues the MMAs at the
+//     widest shape (N = 256 columns per chunk): D goes to one of two
+//     256-column TMEM buffers;
 //   * warps 1-4 stage the next tile's limbs into a two-slot ring in the MMA's
-//     K-major layout (coalesced 16-byte loads, conflict-free stores thanks to a
-//     padded K stride) while the current tile is multiplied and folded;
+//     K-major layout while the current tile is multiplied and folded: a warp
+//     moves 8 rows x 4 sixteen-byte groups at a time, so the global loads are
+//     64-byte runs and the eight lanes of each shared-store phase hit eight
+//     different bank groups;
 //   * warps 5-20, four per TMEM lane quadrant, one coefficient per thread,
-//     each take 8 of a chunk's 32 primes: read D, fold the 49-bit sums mod p_j
-//     and store the residues (a warp writes 32 consecutive words per prime).
+//     each take 16 of a chunk's 64 primes: read D, fold the 49-bit sums mod
+//     p_j and store the residues (a warp writes 32 consecutive words per
+//     prime).
 // The fold constants come from kernel parameters.  Every wait is bounded; a
 // timeout raises an abort flag that every role checks, and the error word gets
 // bit 0.
@@ -35,12 +39,16 @@ constexpr int kLoaders = 128;
 constexpr int kEpiWarp0 = 5;                       // warps 5-20
 constexpr int kEpi = 512;
 constexpr uint32_t kRows = 128;
-constexpr uint32_t kCols = 128;                    // GEMM columns per chunk (32 primes)
-constexpr uint32_t kALbo = kRows * 16 + 16;        // K stride of the operand tile, padded
+constexpr uint32_t kCols = 256;                    // GEMM columns per full chunk (64 primes)
+constexpr uint32_t kALbo = kRows * 16;             // K stride of the operand tile (128-byte aligned)
 
 __host__ __device__ inline uint32_t a_bytes(uint32_t kb) { return (kb / 16) * kALbo; }
-__host__ __device__ inline size_t b_bytes(uint32_t kb, int nch) { return static_cast<size_t>(nch) * kCols * kb; }
-__host__ inline size_t smem_bytes(uint32_t kb, int nch) { return b_bytes(kb, nch) + 2 * a_bytes(kb) + 128; }
+__host__ __device__ inline size_t b_bytes(uint32_t kb, int nch, uint32_t nlast) {
+    return (static_cast<size_t>(nch) - 1) * kCols * kb + static_cast<size_t>(nlast) * kb;
+}
+__host__ inline size_t smem_bytes(uint32_t kb, int nch, uint32_t nlast) {
+    return b_bytes(kb, nch, nlast) + 2 * a_bytes(kb) + 128;
+}
 
 struct Smem {
     uint8_t* b;            // resident constant image
@@ -48,23 +56,23 @@ struct Smem {
     uint64_t* b_full;      // [1]
     uint64_t* a_full;      // [2]
     uint64_t* a_empty;     // [2]
-    uint64_t* d_full;      // [4]
-    uint64_t* d_empty;     // [4]
+    uint64_t* d_full;      // [2]
+    uint64_t* d_empty;     // [2]
     uint32_t* tmem_base;
     volatile uint32_t* abort;
 };
 
-__device__ inline Smem carve(uint8_t* base, uint32_t kb, int nch) {
+__device__ inline Smem carve(uint8_t* base, uint32_t kb, int nch, uint32_t nlast) {
     Smem s;
     s.b = base;
-    s.a = base + b_bytes(kb, nch);
+    s.a = base + b_bytes(kb, nch, nlast);
     uint64_t* bars = reinterpret_cast<uint64_t*>(s.a + 2 * a_bytes(kb));
     s.b_full = bars;
     s.a_full = bars + 1;
     s.a_empty = bars + 3;
     s.d_full = bars + 5;
-    s.d_empty = bars + 9;
-    s.tmem_base = reinterpret_cast<uint32_t*>(bars + 13);
+    s.d_empty = bars + 7;
+    s.tmem_base = reinterpret_cast<uint32_t*>(bars + 9);
     s.abort = s.tmem_base + 1;
     return s;
 }
@@ -98,15 +106,16 @@ __global__ void __launch_bounds__(kThreads, 1)
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     pdl_launch_dependents();
     const uint32_t kb = d.dec_kb;
-    const int nch = d.dec_chunks;
-    const Smem sm = carve(smem_raw, kb, nch);
+    const int nch = static_cast<int>(fc.chunks);
+    const uint32_t nlast = fc.last_cols;
+    const Smem sm = carve(smem_raw, kb, nch, nlast);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int L = d.L, K = d.K;
     const bool second = blockIdx.x >= split;
     const int operand = operand0 + (second ? 1 : 0);
     const uint32_t* limbs = second ? lb : la;
     uint32_t* res = second ? rb : ra;
-    const uint8_t* img = operand ? d.dec_img_b : d.dec_img_a;
+    const uint8_t* img = fc.img[operand];
     const uint32_t g0 = second ? split : 0, gs = second ? gridDim.x - split : split;
     const uint32_t tiles = (n_end - n_begin + kRows - 1) / kRows;
     const uint32_t chunk_bytes = kCols * kb;
@@ -117,7 +126,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc::mbar_init(&sm.a_full[i], kLoaders);
             tc::mbar_init(&sm.a_empty[i], 1);
         }
-        for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < 2; ++i) {
             tc::mbar_init(&sm.d_full[i], 1);
             tc::mbar_init(&sm.d_empty[i], kEpi);
         }
@@ -125,9 +134,12 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc::fence_mbar_init();
         // The constant image is read-only plan data: it loads under the
         // preceding kernel's tail.
-        tc::mbar_arrive_expect_tx(sm.b_full, static_cast<uint32_t>(b_bytes(kb, nch)));
-        for (int c = 0; c < nch; ++c)
-            tc::bulk_g2s(sm.b + c * chunk_bytes, img + static_cast<size_t>(c) * chunk_bytes, chunk_bytes, sm.b_full);
+        const uint32_t total = static_cast<uint32_t>(b_bytes(kb, nch, nlast));
+        tc::mbar_arrive_expect_tx(sm.b_full, total);
+        for (uint32_t off = 0; off < total; off += chunk_bytes) {
+            const uint32_t n = total - off < chunk_bytes ? total - off : chunk_bytes;
+            tc::bulk_g2s(sm.b + off, img + off, n, sm.b_full);
+        }
     }
     if (warp == 0) tc::tmem_alloc(sm.tmem_base, 512);
     tc::tc_fence_before();
@@ -139,7 +151,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (warp == 0) {
         // ---- MMA issuer ----
         if (lane == 0) {
-            const uint32_t idesc = tc::idesc_u8(kCols);
+            const uint32_t idesc_full = tc::idesc_u8(kCols), idesc_last = tc::idesc_u8(nlast);
             bool ok = wait_or_abort(sm.b_full, 0, sm.abort);
             uint64_t* last_bar = nullptr;   // the barrier of the latest commit
             uint32_t last_par = 0;
@@ -150,21 +162,23 @@ __global__ void __launch_bounds__(kThreads, 1)
                 if (!ok) break;
                 const uint32_t a0 = tc::smem_addr(sm.a + s * a_bytes(kb));
                 for (int c = 0; c < nch; ++c, ++g) {
-                    const int buf = g & 3;
-                    if (g >= 4) {
-                        ok = wait_or_abort(&sm.d_empty[buf], ((g - 4) >> 2) & 1, sm.abort);
+                    const int buf = g & 1;
+                    if (g >= 2) {
+                        ok = wait_or_abort(&sm.d_empty[buf], ((g - 2) >> 1) & 1, sm.abort);
                         if (!ok) break;
                     }
                     tc::tc_fence_after();
+                    const bool lastc = c == nch - 1;
+                    const uint32_t cols = lastc ? nlast : kCols;
                     const uint32_t b0 = tc::smem_addr(sm.b + c * chunk_bytes);
                     for (uint32_t kk = 0; kk < kb / 32; ++kk) {
                         const uint64_t ad = tc::smem_desc(a0 + kk * 2 * kALbo, kALbo, 128);
-                        const uint64_t bd = tc::smem_desc(b0 + kk * 2 * (kCols * 16), kCols * 16, 128);
-                        tc::mma_u8(tmem + buf * kCols, ad, bd, idesc, kk > 0);
+                        const uint64_t bd = tc::smem_desc(b0 + kk * 2 * (cols * 16), cols * 16, 128);
+                        tc::mma_u8(tmem + buf * kCols, ad, bd, lastc ? idesc_last : idesc_full, kk > 0);
                     }
                     tc::mma_commit(&sm.d_full[buf]);
                     last_bar = &sm.d_full[buf];
-                    last_par = (g >> 2) & 1;
+                    last_par = (g >> 1) & 1;
                 }
                 if (!ok) break;
                 tc::mma_commit(&sm.a_empty[s]);
@@ -194,20 +208,25 @@ __global__ void __launch_bounds__(kThreads, 1)
             // Every position of the tile is written once: a limb, or zero for
             // rows past nk and limbs past L.
             if (vec) {
-                // 16-byte group gq of row m is limbs 4 gq .. 4 gq + 3.
-                const uint32_t q4 = static_cast<uint32_t>(L) / 4, G = kb / 16, n16 = kRows * G;
+                // 16-byte group gq of row m is limbs 4 gq .. 4 gq + 3; block
+                // (mb, gb) is rows 8 mb .. + 7 and groups 4 gb .. + 3.
+                const uint32_t q4 = static_cast<uint32_t>(L) / 4, G = kb / 16, gbs = (G + 3) / 4;
+                const uint32_t nblk = (kRows / 8) * gbs, lw = lt >> 5;
+                const uint32_t r = lane & 7, gi = lane >> 3;
                 const uint4* src4 = reinterpret_cast<const uint4*>(limbs + static_cast<size_t>(n0) * L);
-                for (uint32_t w0 = lt; w0 < n16; w0 += 8 * kLoaders) {
+                for (uint32_t b0 = lw; b0 < nblk; b0 += 8 * (kLoaders / 32)) {
                     uint4 v[8];
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
-                        const uint32_t w = w0 + k * kLoaders, mm = w / G, gq = w - mm * G;
-                        v[k] = (w < n16 && mm < nk && gq < q4) ? __ldg(src4 + mm * q4 + gq) : make_uint4(0, 0, 0, 0);
+                        const uint32_t blk = b0 + k * (kLoaders / 32), mb = blk / gbs, gb = blk - mb * gbs;
+                        const uint32_t mm = 8 * mb + r, gq = 4 * gb + gi;
+                        v[k] = (blk < nblk && mm < nk && gq < q4) ? __ldg(src4 + mm * q4 + gq) : make_uint4(0, 0, 0, 0);
                     }
 #pragma unroll
                     for (int k = 0; k < 8; ++k) {
-                        const uint32_t w = w0 + k * kLoaders, mm = w / G, gq = w - mm * G;
-                        if (w < n16) *reinterpret_cast<uint4*>(at + gq * kALbo + mm * 16) = v[k];
+                        const uint32_t blk = b0 + k * (kLoaders / 32), mb = blk / gbs, gb = blk - mb * gbs;
+                        const uint32_t mm = 8 * mb + r, gq = 4 * gb + gi;
+                        if (blk < nblk && gq < G) *reinterpret_cast<uint4*>(at + gq * kALbo + mm * 16) = v[k];
                     }
                 }
             } else {
@@ -222,35 +241,36 @@ __global__ void __launch_bounds__(kThreads, 1)
             tc::mbar_arrive(&sm.a_full[s]);
         }
     } else {
-        // ---- epilogue: thread = one coefficient, 8 primes of each chunk ----
+        // ---- epilogue: thread = one coefficient, 16 primes of each chunk ----
         const int ew = warp - kEpiWarp0;
         const uint32_t qd = warp & 3, piece = ew >> 2;
         const uint32_t m = qd * 32 + lane;
-        const uint32_t tq = tmem + ((qd * 32) << 16) + piece * 32;
+        const uint32_t tq = tmem + ((qd * 32) << 16) + piece * 64;
         uint32_t g = 0;
         for (uint32_t t = blockIdx.x - g0; t < tiles; t += gs) {
             const uint32_t n0 = n_begin + t * kRows;
             const bool live = m < min(kRows, n_end - n0);
             bool ok = true;
             for (int c = 0; c < nch; ++c, ++g) {
-                const int buf = g & 3;
-                ok = wait_or_abort(&sm.d_full[buf], (g >> 2) & 1, sm.abort);
+                const int buf = g & 1;
+                ok = wait_or_abort(&sm.d_full[buf], (g >> 1) & 1, sm.abort);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
                 tc::tc_fence_after();
-                const int j0 = c * 32 + static_cast<int>(piece) * 8;
-                uint32_t r[32];
-                tc::tmem_ld32(tq + buf * kCols, r);
+                const int j0 = c * 64 + static_cast<int>(piece) * 16;
+                uint32_t r[2][32];
+                tc::tmem_ld32(tq + buf * kCols, r[0]);
+                tc::tmem_ld32(tq + buf * kCols + 32, r[1]);
                 tc::tmem_ld_wait();
                 tc::tc_fence_before();
                 tc::mbar_arrive(&sm.d_empty[buf]);
                 if (j0 < K) {
 #pragma unroll
-                    for (int k = 0; k < 8; ++k) {
+                    for (int k = 0; k < 16; ++k) {
                         const int j = j0 + k;
-                        const uint64_t v = static_cast<uint64_t>(r[4 * k]) + (static_cast<uint64_t>(r[4 * k + 1]) << 8) +
-                                           (static_cast<uint64_t>(r[4 * k + 2]) << 16) +
-                                           (static_cast<uint64_t>(r[4 * k + 3]) << 24);
+                        const uint32_t* rr = r[k >> 3] + 4 * (k & 7);
+                        const uint64_t v = static_cast<uint64_t>(rr[0]) + (static_cast<uint64_t>(rr[1]) << 8) +
+                                           (static_cast<uint64_t>(rr[2]) << 16) + (static_cast<uint64_t>(rr[3]) << 24);
                         if (live && j < K) res[static_cast<size_t>(j) * d.N + n0 + m] = fold49(v, fc.fold[j]);
                     }
                 }
@@ -270,15 +290,19 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 }  // namespace
 
-DecConsts make_dec_consts(const HostPlan& pl) {
+DecConsts make_dec_consts(const HostPlan& pl, const uint8_t* img_a, const uint8_t* img_b) {
     DecConsts dc{};
     for (int j = 0; j < pl.K; ++j) dc.fold[j] = pl.dec_fold[j];
+    dc.img[0] = img_a;
+    dc.img[1] = img_b;
+    dc.chunks = pl.dec_wchunks;
+    dc.last_cols = pl.dec_wlast;
     return dc;
 }
 
-bool decompose_pipe_supported(const DevPoint& d) {
-    return d.dec_chunks >= 1 && d.dec_chunks <= static_cast<int>(kMaxK / 32) && d.K <= kMaxK &&
-           smem_bytes(d.dec_kb, d.dec_chunks) <= 227 * 1024;
+bool decompose_pipe_supported(const HostPlan& pl) {
+    return pl.K <= kMaxK && pl.dec_wchunks >= 1 && pl.dec_wlast >= 16 && pl.dec_wlast <= 256 &&
+           smem_bytes(pl.dec_kb, static_cast<int>(pl.dec_wchunks), pl.dec_wlast) <= 227 * 1024;
 }
 
 void decompose_pipe_init_attributes() {
@@ -298,7 +322,8 @@ void launch_decompose_pipe(const DevPoint& d, const DecConsts& dc, const uint32_
     if (per > tiles) per = tiles;
     const uint32_t grid = per * operands;
     const uint32_t split = operands == 2 ? per : grid;
-    check(launch_pdl(k_decompose_pipe, dim3(grid), dim3(kThreads), smem_bytes(d.dec_kb, d.dec_chunks), st, d, dc, a,
+    check(launch_pdl(k_decompose_pipe, dim3(grid), dim3(kThreads),
+                     smem_bytes(d.dec_kb, static_cast<int>(dc.chunks), dc.last_cols), st, d, dc, a,
                      b ? b : a, A, B ? B : A, operand0, n_begin, n_end, split),
           "decompose launch");
 }

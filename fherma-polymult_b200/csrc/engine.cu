@@ -89,7 +89,11 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
         dp_.crt_img_v = upload(pl.crt_img_v);
         dp_.negp_top = pl.negp_top;
         if (crt_uses_tc(pl)) crt_consts_.reset(new CrtConsts(make_crt_consts(pl)));
-        if (decompose_pipe_supported(dp_)) dec_consts_.reset(new DecConsts(make_dec_consts(pl)));
+        if (decompose_pipe_supported(pl)) {
+            const uint8_t* wa = upload(pl.dec_wimg_a);
+            const uint8_t* wb = upload(pl.dec_wimg_b);
+            dec_consts_.reset(new DecConsts(make_dec_consts(pl, wa, wb)));
+        }
         dp_.err = dalloc<uint32_t>(1);
         check(cudaMemset(dp_.err, 0, sizeof(uint32_t)), "memset");
         if (const char* k = std::getenv("FPM_KERNELS")) simt_ = std::strcmp(k, "simt") == 0;

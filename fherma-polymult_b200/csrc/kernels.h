@@ -81,9 +81,12 @@ void launch_crt_pipe(const DevPoint& d, const CrtConsts& cc, const uint32_t* Y, 
 // otherwise all take a -> A as operand `operand0`.
 struct DecConsts {
     uint4 fold[kMaxK];          // {p, 2^32 mod p, its Shoup companion, floor(2^32 / p)}
+    const uint8_t* img[2];      // device copies of the plan's wide images, operands a and b
+    uint32_t chunks;            // chunks of 64 primes
+    uint32_t last_cols;         // GEMM columns of the last chunk
 };
-DecConsts make_dec_consts(const HostPlan& pl);
-bool decompose_pipe_supported(const DevPoint& d);
+DecConsts make_dec_consts(const HostPlan& pl, const uint8_t* img_a, const uint8_t* img_b);
+bool decompose_pipe_supported(const HostPlan& pl);
 void decompose_pipe_init_attributes();
 void launch_decompose_pipe(const DevPoint& d, const DecConsts& dc, const uint32_t* a, const uint32_t* b,
                            uint32_t* A, uint32_t* B, int operand0, uint32_t n_begin, uint32_t n_end, int sms,

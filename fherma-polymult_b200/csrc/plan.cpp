@@ -97,6 +97,7 @@ size_t device_footprint(const HostPlan& pl) {
                bytes(pl.row_u_f) + bytes(pl.row_q_f) +
                bytes(pl.full_f) + bytes(pl.full_i) + bytes(pl.q) + bytes(pl.M) + bytes(pl.negvP) +
                bytes(pl.p_recip) + bytes(pl.dec_img_a) + bytes(pl.dec_img_b) + bytes(pl.dec_fold) +
+               bytes(pl.dec_wimg_a) + bytes(pl.dec_wimg_b) +
                bytes(pl.crt_img) + bytes(pl.crt_img_v) + sizeof(uint32_t);
     t += 2 * static_cast<size_t>(pl.K) * pl.N * sizeof(uint32_t);   // residue workspaces
     t += 3 * static_cast<size_t>(pl.N) * pl.L * sizeof(uint32_t);   // host-path limb buffers
@@ -242,6 +243,13 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
     pl.dec_img_a.assign(dchunk * pl.dec_chunks, 0);
     pl.dec_img_b.assign(dchunk * pl.dec_chunks, 0);
     pl.dec_fold.resize(K);
+    // Wide images: chunks of 64 primes (256 GEMM columns, the MMA's widest N);
+    // the last chunk packed to its own width, a multiple of 16 columns.
+    pl.dec_wchunks = static_cast<uint32_t>((K + 63) / 64);
+    pl.dec_wlast = (4 * static_cast<uint32_t>(K - 64 * (static_cast<int>(pl.dec_wchunks) - 1)) + 15) / 16 * 16;
+    const size_t wchunk = static_cast<size_t>(256) * pl.dec_kb;
+    pl.dec_wimg_a.assign(wchunk * (pl.dec_wchunks - 1) + static_cast<size_t>(pl.dec_wlast) * pl.dec_kb, 0);
+    pl.dec_wimg_b.assign(pl.dec_wimg_a.size(), 0);
     for (int j = 0; j < K; ++j) {
         const uint32_t p = pl.primes[j];
         const uint32_t r32 = static_cast<uint32_t>((1ull << 32) % p);
@@ -256,6 +264,11 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
                 const size_t at = chunk + (k / 16) * (128 * 16) + col * 16 + (k % 16);
                 pl.dec_img_a[at] = static_cast<uint8_t>(ca >> (8 * s));
                 pl.dec_img_b[at] = static_cast<uint8_t>(cb >> (8 * s));
+                const uint32_t wc = static_cast<uint32_t>(j / 64), wcol = 4 * (j % 64) + s;
+                const uint32_t wcols = wc + 1 < pl.dec_wchunks ? 256 : pl.dec_wlast;
+                const size_t wat = wc * wchunk + (k / 16) * (wcols * 16) + wcol * 16 + (k % 16);
+                pl.dec_wimg_a[wat] = static_cast<uint8_t>(ca >> (8 * s));
+                pl.dec_wimg_b[wat] = static_cast<uint8_t>(cb >> (8 * s));
             }
         }
     }

@@ -78,6 +78,10 @@ struct HostPlan {
     uint32_t dec_kb = 0;                     // GEMM K in bytes: 4L rounded up to 32
     uint32_t dec_chunks = 0;                 // ceil(K / 32)
     std::vector<uint8_t> dec_img_a, dec_img_b;
+    // The same constants in chunks of 64 primes (256 columns) for the
+    // pipelined decompose; the last chunk has dec_wlast columns.
+    uint32_t dec_wchunks = 0, dec_wlast = 0;
+    std::vector<uint8_t> dec_wimg_a, dec_wimg_b;
     std::vector<uint4> dec_fold;             // K: {p, 2^32 mod p, its Shoup companion, floor(2^32 / p)}
 
     // Tensor-core CRT (crt_tc.cu), L >= 2: B operand, row u (a byte position of
