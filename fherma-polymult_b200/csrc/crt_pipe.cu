@@ -116,7 +116,7 @@ __device__ __forceinline__ uint32_t ld_stream(const uint32_t* p) {
 __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile uint32_t* abort) {
     if (tc::mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = tc::globaltimer();
-    while (!tc::mbar_try_wait(bar, parity)) {
+    while (!tc::mbar_try_wait_sleep(bar, parity)) {
         if (*abort) return false;
         if (tc::globaltimer() - t0 > tc::kWaitNs) {
             *abort = 1;

@@ -54,11 +54,25 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
+// As mbar_try_wait, but the thread may sleep in hardware (up to about
+// kSuspendNs) until the phase completes, instead of spinning.
+constexpr uint32_t kSuspendNs = 500000;
+
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{ .reg .pred P; mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2, %3; selp.u32 %0, 1, 0, P; }"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(kSuspendNs)
+        : "memory");
+    return ok != 0;
+}
+
 // Waits for the phase with the given parity to complete; false on timeout.
 __device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer();
-    while (!mbar_try_wait(bar, parity)) {
+    while (!mbar_try_wait_sleep(bar, parity)) {
         if (globaltimer() - t0 > kWaitNs) return false;
     }
     return true;
