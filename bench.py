@@ -56,7 +56,7 @@ ROTATE = 4
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="N65536_W2048")
@@ -91,53 +91,70 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+    """SM clocks and clock-event (throttle) reasons, read through NVML every
+    5 ms on a background thread while the timed region runs (the same data as
+    nvidia-smi's clocks.sm and clocks_event_reasons.* queries)."""
+
+    NAMES = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+             "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+             "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+             "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
 
     def __init__(self, index: int):
-        self.index = index
-        self.proc = None
-        self.path = None
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [x.strip() for x in vis.split(",") if x.strip()]
+        self.index = int(ids[index]) if index < len(ids) and ids[index].isdigit() else index
+        self.sm, self.smax, self.reasons = [], 0.0, set()
+        self.error = None
+        self._stop = None
+        self._thread = None
+
+    def _run(self):
+        import pynvml
+        h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+        self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        bits = {name: getattr(pynvml, const) for name, const in self.NAMES.items()}
+        while not self._stop.is_set():
+            self.sm.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+            r = get_reasons(h)
+            for name, bit in bits.items():
+                if r & bit:
+                    self.reasons.add(name)
+            self._stop.wait(0.005)
 
     def __enter__(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
-        time.sleep(0.3)
+            import pynvml
+            pynvml.nvmlInit()
+        except Exception as e:   # the record is reported, not required
+            self.error = str(e)
+            return self
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._guarded, daemon=True)
+        self._thread.start()
+        time.sleep(0.02)
         return self
 
+    def _guarded(self):
+        try:
+            self._run()
+        except Exception as e:
+            self.error = str(e)
+
     def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            self.proc.wait()
+        if self._thread:
+            self._stop.set()
+            self._thread.join()
 
     def summary(self):
-        sm, smax, reasons = [], 0.0, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        try:
-            for line in open(self.path):
-                f = [x.strip() for x in line.split(",")]
-                if len(f) < 9:
-                    continue
-                try:
-                    sm.append(float(f[1]))
-                    smax = max(smax, float(f[2]))
-                except ValueError:
-                    continue
-                for name, v in zip(names, f[5:9]):
-                    if v.lower().startswith("active"):
-                        reasons.add(name)
-        finally:
-            os.unlink(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax or None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        out = {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.smax or None,
+               "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "NVML, 5 ms"}
+        if self.error:
+            out["error"] = self.error
+        return out
 
 
 def algorithmic_bytes(N, L, K):
@@ -418,7 +435,9 @@ def main():
     stages["transform"] = time_stage(lambda: ctx.stage_transform(A.data_ptr(), B.data_ptr(), 0, sp))
     stages["crt"] = time_stage(lambda: ctx.stage_crt(A.data_ptr(), dc.data_ptr(), sp))
     # One kernel at a time (the transform's passes alone: modes 2, 3, 4).
-    kernels = {"k_decompose_tc": stages["decompose"], "k_crt_tc": stages["crt"]}
+    # Decompose and CRT: the persistent pipelines; the decompose stage is one
+    # operand's launch (a product's single paired launch does both).
+    kernels = {"k_decompose_pipe": stages["decompose"], "k_crt_pipe": stages["crt"]}
     if ctx.info.logR:
         kernels["k_ntt_col_fwd"] = time_stage(lambda: ctx.stage_transform(A.data_ptr(), B.data_ptr(), 2, sp))
         kernels["k_ntt_col_inv"] = time_stage(lambda: ctx.stage_transform(A.data_ptr(), B.data_ptr(), 4, sp))
@@ -476,10 +495,10 @@ def main():
 
     hbm, peak_kind = peaks()
     ab = algorithmic_bytes(N, L, K)
-    kernel_bytes = {"k_decompose_tc": ab["decompose"], "k_ntt_col_fwd": ab["ntt_col_fwd"], "k_ntt_row": ab["ntt_row"],
-                    "k_ntt_col_inv": ab["ntt_col_inv"], "k_crt_tc": ab["crt"]}
+    kernel_bytes = {"k_decompose_pipe": ab["decompose"], "k_ntt_col_fwd": ab["ntt_col_fwd"],
+                    "k_ntt_row": ab["ntt_row"], "k_ntt_col_inv": ab["ntt_col_inv"], "k_crt_pipe": ab["crt"]}
     # launches per product: the dominant kernel's time share in one product
-    per_product = {"k_decompose_tc": 2, "k_ntt_col_fwd": 1, "k_ntt_row": 1, "k_ntt_col_inv": 1, "k_crt_tc": 1}
+    per_product = {"k_decompose_pipe": 2, "k_ntt_col_fwd": 1, "k_ntt_row": 1, "k_ntt_col_inv": 1, "k_crt_pipe": 1}
     dom = max(kernels, key=lambda k: kernels[k] * per_product[k])
     achieved = kernel_bytes[dom] / (kernels[dom] * 1e-6) / 1e9
     traffic = None
