@@ -174,6 +174,15 @@ def algorithmic_bytes(N, L, K):
     }
 
 
+def job_time(ms_local: float, steps: int, world: int, reduce_max):
+    """Whole-job time of a replica run: every rank multiplies `steps` products
+    of its own, so the job takes as long as the slowest rank (max over ranks of
+    the device time) and the value is that time over all ranks' products.
+    Returns (ms, us per product)."""
+    ms = float(reduce_max(ms_local)) if world > 1 else float(ms_local)
+    return ms, ms * 1e3 / (steps * world)
+
+
 def run_reference(args):
     """The reference's own CPU implementation (solve_cpu.cpp via the shim in
     oracle/_ref/libref_cpu.so), all host threads, same workload and metric."""
@@ -458,14 +467,14 @@ def main():
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    ms = start.elapsed_time(end)
     clocks = clk.summary()
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
+
+    def reduce_max(v):
+        t = torch.tensor([v], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    products = args.steps * world
-    us_per_product = ms * 1e3 / products
+        return t.item()
+
+    ms, us_per_product = job_time(start.elapsed_time(end), args.steps, world, reduce_max)
 
     # End to end through the C API with host buffers (fpm_run): pinned buffers
     # (the headline: host->device copies of a and b and the device->host copy of
