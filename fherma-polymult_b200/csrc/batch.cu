@@ -258,11 +258,15 @@ Batch::Batch(const std::vector<Engine*>& engines) {
             prods_.push_back(p);
         }
         check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "stream");
+        check(cudaStreamCreateWithFlags(&copy_, cudaStreamNonBlocking), "stream");
+        check(cudaStreamCreateWithFlags(&out_, cudaStreamNonBlocking), "stream");
         build_graph();
     } catch (...) {
         release_graph();
         for (auto s : branches_) cudaStreamDestroy(s);
         for (auto ev : events_) cudaEventDestroy(ev);
+        for (cudaStream_t x : {copy_, out_})
+            if (x) cudaStreamDestroy(x);
         if (stream_) cudaStreamDestroy(stream_);
         if (slab_) cudaFree(slab_);
         throw;
@@ -270,10 +274,14 @@ Batch::Batch(const std::vector<Engine*>& engines) {
 }
 
 Batch::~Batch() {
-    if (stream_) cudaStreamSynchronize(stream_);
+    for (cudaStream_t x : {copy_, out_, stream_})
+        if (x) cudaStreamSynchronize(x);
     release_graph();
     for (auto s : branches_) cudaStreamDestroy(s);
     for (auto ev : events_) cudaEventDestroy(ev);
+    for (auto ev : io_events_) cudaEventDestroy(ev);
+    for (cudaStream_t x : {copy_, out_})
+        if (x) cudaStreamDestroy(x);
     if (stream_) cudaStreamDestroy(stream_);
     if (slab_) cudaFree(slab_);
 }
@@ -281,6 +289,9 @@ Batch::~Batch() {
 void Batch::release_graph() {
     if (exec_) cudaGraphExecDestroy(exec_);
     exec_ = nullptr;
+    for (cudaGraphExec_t e : io_exec_) cudaGraphExecDestroy(e);
+    io_exec_.clear();
+    io_groups_.clear();
 }
 
 cudaStream_t Batch::branch(size_t i) {
@@ -326,10 +337,20 @@ void Batch::build_graph() {
         }
     }
     for (size_t i = 0; i < classes; ++i) branch(i);
+    exec_ = capture(prods_, &launches_);
+}
+
+cudaGraphExec_t Batch::capture(const std::vector<GroupedProduct>& prods, int* launches) {
+    GroupedLaunchEnv env;
+    env.branches = branches_;
+    env.events = events_;
+    env.occupancy = &occupancy_;
+    env.sms = sms_;
     cudaGraph_t graph = nullptr;
     check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "begin capture");
     try {
-        enqueue(stream_);
+        const int n = enqueue_grouped(prods, sched_, stream_, env);
+        if (launches) *launches = n;
     } catch (...) {
         cudaStreamEndCapture(stream_, &graph);
         if (graph) cudaGraphDestroy(graph);
@@ -337,33 +358,70 @@ void Batch::build_graph() {
         throw;
     }
     check(cudaStreamEndCapture(stream_, &graph), "end capture");
-    const cudaError_t e = cudaGraphInstantiate(&exec_, graph, 0);
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     check(e, "graph instantiate");
+    return exec;
 }
 
-void Batch::enqueue(cudaStream_t st) {
-    GroupedLaunchEnv env;
-    env.branches = branches_;
-    env.events = events_;
-    env.occupancy = &occupancy_;
-    env.sms = sms_;
-    launches_ = enqueue_grouped(prods_, sched_, st, env);
+// Sub-batches for the host path: the products in schedule order, cut into up
+// to kIoGroups runs of about equal work, each captured as its own graph.
+void Batch::build_io_graphs() {
+    if (!io_exec_.empty()) return;
+    std::vector<size_t> ord(prods_.size());
+    std::iota(ord.begin(), ord.end(), size_t(0));
+    if (sched_.order == 1) {
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t x, size_t y) { return prods_[x].cost > prods_[y].cost; });
+    }
+    double total = 0;
+    for (const GroupedProduct& p : prods_) total += p.cost;
+    const size_t groups = std::min<size_t>(kIoGroups, prods_.size());
+    io_groups_.assign(1, {});
+    double acc = 0;
+    for (size_t k = 0; k < ord.size(); ++k) {
+        io_groups_.back().push_back(ord[k]);
+        acc += prods_[ord[k]].cost;
+        const size_t left = ord.size() - k - 1;
+        if (io_groups_.size() < groups && left > 0 && acc >= total * io_groups_.size() / groups)
+            io_groups_.emplace_back();
+    }
+    for (const std::vector<size_t>& g : io_groups_) {
+        std::vector<GroupedProduct> sub;
+        for (size_t i : g) sub.push_back(prods_[i]);
+        io_exec_.push_back(capture(sub, nullptr));
+    }
+    while (io_events_.size() < 2 * io_groups_.size()) {
+        cudaEvent_t ev = nullptr;
+        check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+        io_events_.push_back(ev);
+    }
 }
 
 void Batch::run_device(cudaStream_t st) { check(cudaGraphLaunch(exec_, st), "graph launch"); }
 
 void Batch::run_host(const uint32_t* const* a, const uint32_t* const* b, uint32_t* const* c) {
-    for (size_t i = 0; i < prods_.size(); ++i) {
-        const size_t bytes = prods_[i].e->words() * 4;
-        check(cudaMemcpyAsync(prods_[i].a, a[i], bytes, cudaMemcpyHostToDevice, stream_), "copy a");
-        check(cudaMemcpyAsync(prods_[i].b, b[i], bytes, cudaMemcpyHostToDevice, stream_), "copy b");
+    build_io_graphs();
+    // Sub-batch s: its copies in (copy stream), its graph (compute stream),
+    // its copies out (out stream); s + 1 moves in while s computes and s - 1
+    // moves out.
+    for (size_t s = 0; s < io_groups_.size(); ++s) {
+        for (size_t i : io_groups_[s]) {
+            const size_t bytes = prods_[i].e->words() * 4;
+            check(cudaMemcpyAsync(prods_[i].a, a[i], bytes, cudaMemcpyHostToDevice, copy_), "copy a");
+            check(cudaMemcpyAsync(prods_[i].b, b[i], bytes, cudaMemcpyHostToDevice, copy_), "copy b");
+        }
+        check(cudaEventRecord(io_events_[2 * s], copy_), "event record");
+        check(cudaStreamWaitEvent(stream_, io_events_[2 * s], 0), "stream wait");
+        check(cudaGraphLaunch(io_exec_[s], stream_), "graph launch");
+        check(cudaEventRecord(io_events_[2 * s + 1], stream_), "event record");
+        check(cudaStreamWaitEvent(out_, io_events_[2 * s + 1], 0), "stream wait");
+        for (size_t i : io_groups_[s]) {
+            const size_t bytes = prods_[i].e->words() * 4;
+            check(cudaMemcpyAsync(c[i], prods_[i].c, bytes, cudaMemcpyDeviceToHost, out_), "copy c");
+        }
     }
-    run_device(stream_);
-    for (size_t i = 0; i < prods_.size(); ++i) {
-        const size_t bytes = prods_[i].e->words() * 4;
-        check(cudaMemcpyAsync(c[i], prods_[i].c, bytes, cudaMemcpyDeviceToHost, stream_), "copy c");
-    }
+    check(cudaStreamSynchronize(out_), "batch sync");
     check(cudaStreamSynchronize(stream_), "batch sync");
     if (take_error()) throw std::runtime_error("batch: a tensor-core pipeline wait timed out");
 }

@@ -83,7 +83,8 @@ public:
     // Every product of the batch on its device buffers: one graph launch on st.
     void run_device(cudaStream_t st);
     // The same from host arrays (a[i], b[i] in, c[i] out); returns when every
-    // c[i] is written.
+    // c[i] is written.  The products run as up to four sub-batches (separate
+    // graphs) so each one's copies overlap the others' kernels.
     void run_host(const uint32_t* const* a, const uint32_t* const* b, uint32_t* const* c);
 
     // Times each candidate schedule (one warm-up and `reps` timed graph
@@ -98,8 +99,9 @@ public:
     uint32_t take_error();
 
 private:
-    void enqueue(cudaStream_t st);
     void build_graph();
+    void build_io_graphs();
+    cudaGraphExec_t capture(const std::vector<GroupedProduct>& prods, int* launches);
     void release_graph();
     cudaStream_t branch(size_t i);
 
@@ -115,6 +117,13 @@ private:
     std::vector<cudaEvent_t> events_;
     std::map<uint64_t, int> occupancy_;   // resident blocks per SM, per grouped transform kernel
     cudaGraphExec_t exec_ = nullptr;
+    // Host path: sub-batches, their graphs, copy streams and events.
+    static constexpr size_t kIoGroups = 4;
+    std::vector<std::vector<size_t>> io_groups_;
+    std::vector<cudaGraphExec_t> io_exec_;
+    std::vector<cudaEvent_t> io_events_;
+    cudaStream_t copy_ = nullptr;
+    cudaStream_t out_ = nullptr;
 };
 
 }  // namespace fpm
