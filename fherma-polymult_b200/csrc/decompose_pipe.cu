@@ -91,14 +91,22 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, vo
 }
 
 // (lo + hi 2^32) mod p for the 49-bit sums: f = {p, 2^32 mod p, its Shoup
-// companion, floor(2^32 / p)}.
+// companion, floor(2^32 / p)}.  LAZY leaves a value below 4p, congruent to
+// the same residue, for a transform whose first butterflies take lazy input.
+template <bool LAZY>
 __device__ __forceinline__ uint32_t fold49(uint64_t v, uint4 f) {
-    const uint32_t lo = shoup(static_cast<uint32_t>(v), 1u, f.w, f.x);
-    const uint32_t hi = shoup(static_cast<uint32_t>(v >> 32), f.y, f.z, f.x);
-    return add_mod(lo, hi, f.x);
+    if constexpr (LAZY) {
+        return shoup_lazy(static_cast<uint32_t>(v), 1u, f.w, f.x) +
+               shoup_lazy(static_cast<uint32_t>(v >> 32), f.y, f.z, f.x);
+    } else {
+        const uint32_t lo = shoup(static_cast<uint32_t>(v), 1u, f.w, f.x);
+        const uint32_t hi = shoup(static_cast<uint32_t>(v >> 32), f.y, f.z, f.x);
+        return add_mod(lo, hi, f.x);
+    }
 }
 
 // CTAs [0, split) take operand 0 (la -> ra), [split, gridDim.x) operand 1.
+template <bool LAZY>
 __global__ void __launch_bounds__(kThreads, 1)
     k_decompose_pipe(DevPoint d, const __grid_constant__ DecConsts fc, const uint32_t* __restrict__ la,
                      const uint32_t* __restrict__ lb, uint32_t* __restrict__ ra, uint32_t* __restrict__ rb,
@@ -271,7 +279,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const uint32_t* rr = r[k >> 3] + 4 * (k & 7);
                         const uint64_t v = static_cast<uint64_t>(rr[0]) + (static_cast<uint64_t>(rr[1]) << 8) +
                                            (static_cast<uint64_t>(rr[2]) << 16) + (static_cast<uint64_t>(rr[3]) << 24);
-                        if (live && j < K) res[static_cast<size_t>(j) * d.N + n0 + m] = fold49(v, fc.fold[j]);
+                        if (live && j < K) res[static_cast<size_t>(j) * d.N + n0 + m] = fold49<LAZY>(v, fc.fold[j]);
                     }
                 }
             }
@@ -297,6 +305,9 @@ DecConsts make_dec_consts(const HostPlan& pl, const uint8_t* img_a, const uint8_
     dc.img[1] = img_b;
     dc.chunks = pl.dec_wchunks;
     dc.last_cols = pl.dec_wlast;
+    // The four-step transforms start with lazy butterflies; the one-block
+    // transform (N <= 1024) and the full-reduction window want canonical input.
+    dc.lazy_out = pl.lazy && pl.g.logN > kSmallLogN ? 1u : 0u;
     return dc;
 }
 
@@ -306,7 +317,9 @@ bool decompose_pipe_supported(const HostPlan& pl) {
 }
 
 void decompose_pipe_init_attributes() {
-    check(cudaFuncSetAttribute(k_decompose_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+    check(cudaFuncSetAttribute(k_decompose_pipe<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+          "decompose_pipe smem");
+    check(cudaFuncSetAttribute(k_decompose_pipe<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
           "decompose_pipe smem");
 }
 
@@ -322,7 +335,7 @@ void launch_decompose_pipe(const DevPoint& d, const DecConsts& dc, const uint32_
     if (per > tiles) per = tiles;
     const uint32_t grid = per * operands;
     const uint32_t split = operands == 2 ? per : grid;
-    check(launch_pdl(k_decompose_pipe, dim3(grid), dim3(kThreads),
+    check(launch_pdl(dc.lazy_out ? k_decompose_pipe<true> : k_decompose_pipe<false>, dim3(grid), dim3(kThreads),
                      smem_bytes(d.dec_kb, static_cast<int>(dc.chunks), dc.last_cols), st, d, dc, a,
                      b ? b : a, A, B ? B : A, operand0, n_begin, n_end, split),
           "decompose launch");

@@ -84,6 +84,7 @@ struct DecConsts {
     const uint8_t* img[2];      // device copies of the plan's wide images, operands a and b
     uint32_t chunks;            // chunks of 64 primes
     uint32_t last_cols;         // GEMM columns of the last chunk
+    uint32_t lazy_out;          // 1: residues below 4p (congruent), for lazy first butterflies
 };
 DecConsts make_dec_consts(const HostPlan& pl, const uint8_t* img_a, const uint8_t* img_b);
 bool decompose_pipe_supported(const HostPlan& pl);

@@ -113,7 +113,10 @@ FPM_API int fpm_get_primes(const fpm_ctx* ctx, uint32_t* out);
  * stage-by-stage checks):
  *   decompose: limbs (N x L) -> residues (K x N, prime-major); operand 0 gives
  *              a mod p_j, operand 1 gives b mod p_j times the pointwise scale
- *              N^-1 (P/p_j)^-1 2^32 (reference k_decompose, solve.cu:98-126);
+ *              N^-1 (P/p_j)^-1 2^32 (reference k_decompose, solve.cu:98-126).
+ *              With 30-bit primes and N > 1024 the values are left below
+ *              4 p_j (congruent; the transform's first butterflies are lazy),
+ *              otherwise they are canonical;
  *   transform: mode 0: A, B -> y_j = INTT(NTT(A) NTT(B)) in A (reference
  *              k_ntt_cols / k_ntt_rows_mul, solve.cu:130-233); mode 1: forward
  *              transforms of A and B in place, bit-reversed order;
