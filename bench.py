@@ -20,7 +20,8 @@ roofline: the dominant kernel's algorithmic bytes per launch over its CUDA-event
 cpu_baseline: the reference's own CPU implementation (solve_cpu.cpp, OpenMP,
          built into oracle/_ref/) on a bounded sample, rank 0 only.
 batched: 64 products of the uneven mix (N 4096 .. 65536, W 128 .. 2048) as one
-         autotuned graph of grouped launches, against 64 sequential plain calls.
+         autotuned graph of grouped launches, against 64 sequential plain calls;
+         batched_n65536: the same for 16 products at N = 65536 (W 1747 / 2048).
 serving: a seeded Poisson stream (10,000 requests at 2000/s) through the
          serving loop; p50 / p99 latency and products/s.
 """
@@ -223,13 +224,25 @@ def pinned_like(torch, x):
     return t, v
 
 
-def measure_batched(torch, polymul, workload, stream, count=64, reps=20):
-    """Batched mix: `count` products, N from {4096 .. 65536} and W from {128 ..
-    2048} (seeded), one graph of grouped launches after the autotuner, against
-    `count` sequential plain calls on the same GPU (device buffers, and host
-    buffers through fpm_run)."""
+def n65536_points(count, seed):
+    """N = 65536 with a 1747-bit or a 2048-bit modulus (alternating), each q
+    seeded: the large single products as a batch."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return [(65536, (1747, 2048)[i % 2], None) for i in range(count)], rng
+
+
+def measure_batched(torch, polymul, workload, stream, count=64, reps=20, mix="uneven"):
+    """Batched mix: `count` products, one graph of grouped launches after the
+    autotuner, against `count` sequential plain calls on the same GPU (device
+    buffers, and host buffers through fpm_run, the reference's fherma_run form).
+    mix "uneven": N from {4096 .. 65536} and W from {128 .. 2048} (seeded);
+    mix "n65536": N = 65536, W alternating 1747 and 2048."""
     sp = stream.cuda_stream
-    pts = workload.mix_points(count, seed=4000)
+    if mix == "n65536":
+        shells, rng = n65536_points(count, seed=3300)
+        pts = [(N, W, workload.random_modulus(W, rng)) for N, W, _ in shells]
+    else:
+        pts = workload.mix_points(count, seed=4000)
     ops = workload.mix_operands(pts, seed=4001)
     ctxs = [polymul.Context(N, W, q) for N, W, q in pts]
     bt = polymul.Batch(ctxs)
@@ -284,14 +297,17 @@ def measure_batched(torch, polymul, workload, stream, count=64, reps=20):
     exact = all(np.array_equal(g, o) for g, o in zip(got, outs)) and all(
         np.array_equal(x, o) for x, o in zip(pc, outs))
     res = {
-        "products": count, "mix": "N in {4096,8192,16384,32768,65536} x W in {128,512,868,1747,2048}, seed 4000",
+        "products": count,
+        "mix": ("N = 65536, W alternating 1747 / 2048, seed 3300" if mix == "n65536" else
+                "N in {4096,8192,16384,32768,65536} x W in {128,512,868,1747,2048}, seed 4000"),
         "batch_us": batch_us, "products_per_s": count / (batch_us * 1e-6),
         "sequential_us": seq_us, "sequential_products_per_s": count / (seq_us * 1e-6),
         "speedup_vs_sequential": seq_us / batch_us,
         "e2e_batch_us": batch_e2e_us, "e2e_sequential_us": seq_e2e_us,
         "e2e_speedup": seq_e2e_us / batch_e2e_us,
+        "device_batch_vs_plain_e2e": seq_e2e_us / batch_us,
         "schedule": {"layout": info.layout, "order": info.order, "prime_group": info.prime_group,
-                     "grid": info.grid, "tuned_us": info.tuned_us},
+                     "grid": info.grid, "pipe_min_log_n": info.pipe_min_log_n, "tuned_us": info.tuned_us},
         "launches_per_batch": info.launches, "device_bytes": info.device_bytes, "bit_exact_vs_plain": bool(exact),
     }
     bt.close()
@@ -535,10 +551,11 @@ def main():
             cpu = {"value": None, "unit": "us/product", "cores": None, "kind": "reference",
                    "sample": f"failed: {e}"}
 
-    batched = serving = None
+    batched = batched_big = serving = None
     if rank == 0 and world == 1:
         if not args.no_batched:
             batched = measure_batched(torch, polymul, workload, stream)
+            batched_big = measure_batched(torch, polymul, workload, stream, count=16, reps=10, mix="n65536")
         if not args.no_serving:
             serving = measure_serving(torch, polymul, workload, n=args.serve_requests, rate=args.serve_rate)
 
@@ -577,6 +594,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
             "batched": batched,
+            "batched_n65536": batched_big,
             "serving": serving,
         }
         print(json.dumps(line))

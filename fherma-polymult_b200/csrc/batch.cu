@@ -75,6 +75,11 @@ int enqueue_grouped(const std::vector<GroupedProduct>& prods_, const BatchSchedu
         }
     }
     TableFill fill;
+    // Large products may take the one-product pipelines for decompose and CRT.
+    auto piped = [&](const GroupedProduct& p) {
+        return sched_.pipe_min_log_n > 0 && static_cast<int>(p.d.logN) >= sched_.pipe_min_log_n &&
+               p.e->dec_consts() != nullptr;
+    };
 
     auto decompose = [&](const std::vector<size_t>& list, cudaStream_t s) {
         fill.reset();
@@ -91,6 +96,11 @@ int enqueue_grouped(const std::vector<GroupedProduct>& prods_, const BatchSchedu
                 launch_decompose(p.d, p.a, p.A, 0, 0, p.d.N, s);
                 launch_decompose(p.d, p.b, p.B, 1, 0, p.d.N, s);
                 launches_ += 2;
+                continue;
+            }
+            if (piped(p)) {
+                launch_decompose_pipe(p.d, *p.e->dec_consts(), p.a, p.b, p.A, p.B, 0, 0, p.d.N, p.e->sms(), s);
+                ++launches_;
                 continue;
             }
             if (fill.full()) flush();
@@ -111,6 +121,11 @@ int enqueue_grouped(const std::vector<GroupedProduct>& prods_, const BatchSchedu
             const GroupedProduct& p = prods_[i];
             if (p.e->simt() || !crt_uses_tc(p.e->plan())) {
                 launch_crt(p.d, p.A, p.c, 0, p.d.N, s);
+                ++launches_;
+                continue;
+            }
+            if (piped(p) && p.e->crt_consts() && crt_pipe_supported(p.d, p.A, 0, p.d.N)) {
+                launch_crt_pipe(p.d, *p.e->crt_consts(), p.A, p.c, 0, p.d.N, p.e->sms(), s);
                 ++launches_;
                 continue;
             }
@@ -304,7 +319,8 @@ cudaStream_t Batch::branch(size_t i) {
 }
 
 void Batch::set_schedule(const BatchSchedule& s) {
-    if (s.layout < 0 || s.layout > 2 || s.order < 0 || s.order > 1 || s.prime_group < 0 || s.grid < 0)
+    if (s.layout < 0 || s.layout > 2 || s.order < 0 || s.order > 1 || s.prime_group < 0 || s.grid < 0 ||
+        s.pipe_min_log_n < 0 || s.pipe_min_log_n > 22)
         throw std::runtime_error("batch: invalid schedule");
     sched_ = s;
     build_graph();
@@ -438,7 +454,8 @@ double Batch::tune(int reps) {
     std::vector<BatchSchedule> cands;
     for (int layout : {0, 1, 2})
         for (int grp : {0, 16})
-            for (int grid : {0, 1}) cands.push_back(BatchSchedule{layout, 1, grp, grid});
+            for (int grid : {0, 1})
+                for (int pipe : {0, 14, 16}) cands.push_back(BatchSchedule{layout, 1, grp, grid, pipe});
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     check(cudaEventCreate(&t0), "event");
     check(cudaEventCreate(&t1), "event");

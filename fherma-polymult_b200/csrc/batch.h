@@ -9,8 +9,9 @@
 // grouped CRT launch, all captured once as a CUDA graph and replayed.
 //
 // The schedule -- whether the geometry chains run as parallel graph branches,
-// the order of the items, how many primes one transform item carries, and
-// whether the transform grids are persistent -- is chosen by Batch::tune,
+// the order of the items, how many primes one transform item carries,
+// whether the transform grids are persistent, and from which size a product
+// takes the one-product pipelines for decompose and CRT -- is chosen by Batch::tune,
 // which times every candidate on this batch and keeps the fastest.
 #pragma once
 
@@ -32,6 +33,8 @@ struct BatchSchedule {
     int prime_group = 0;   // primes per transform item; 0 = all of a product's primes
     int grid = 0;          // transform grids: 0 one block per tile; k > 0 persistent,
                            // k x (resident blocks per SM) x SMs
+    int pipe_min_log_n = 0;   // products with logN >= this (0: none) take the pipelined
+                              // decompose and CRT, one launch each, instead of the grouped ones
 };
 
 // One product of a grouped launch sequence: its point (with the error word

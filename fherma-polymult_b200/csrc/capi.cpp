@@ -225,6 +225,7 @@ int fpm_batch_get_info(const fpm_batch* batch, fpm_batch_info* out) {
     out->order = s.order;
     out->prime_group = s.prime_group;
     out->grid = s.grid;
+    out->pipe_min_log_n = s.pipe_min_log_n;
     out->launches = batch->batch->launches();
     out->device_bytes = batch->batch->device_bytes();
     out->tuned_us = batch->tuned_us;
@@ -238,9 +239,12 @@ int fpm_batch_tune(fpm_batch* batch, int reps, fpm_batch_info* info) {
     return info ? fpm_batch_get_info(batch, info) : FPM_OK;
 }
 
-int fpm_batch_set_schedule(fpm_batch* batch, int layout, int order, int prime_group, int grid) {
+int fpm_batch_set_schedule(fpm_batch* batch, int layout, int order, int prime_group, int grid,
+                           int pipe_min_log_n) {
     if (!batch) return fail(FPM_EINVAL, "fpm_batch_set_schedule: NULL argument");
-    return guarded([&] { batch->batch->set_schedule(fpm::BatchSchedule{layout, order, prime_group, grid}); });
+    return guarded([&] {
+        batch->batch->set_schedule(fpm::BatchSchedule{layout, order, prime_group, grid, pipe_min_log_n});
+    });
 }
 
 void fpm_batch_free(fpm_batch* batch) {

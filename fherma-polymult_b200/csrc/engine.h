@@ -29,6 +29,11 @@ public:
     const DevPoint& point() const { return dp_; }
     int device() const { return device_; }
     bool simt() const { return simt_; }
+    int sms() const { return sms_; }
+    // Kernel parameters of the pipelined decompose and CRT (null where a
+    // point has no pipeline).
+    const DecConsts* dec_consts() const { return dec_consts_.get(); }
+    const CrtConsts* crt_consts() const { return crt_consts_.get(); }
 
     // c = a b on device buffers (N x L each), enqueued on st; the engine's
     // residue workspaces are used, so calls on one engine must not overlap.

@@ -43,7 +43,8 @@ class FpmInfo(ctypes.Structure):
 
 class FpmBatchInfo(ctypes.Structure):
     _fields_ = [("count", ctypes.c_uint32), ("layout", ctypes.c_int32), ("order", ctypes.c_int32),
-                ("prime_group", ctypes.c_int32), ("grid", ctypes.c_int32), ("launches", ctypes.c_int32),
+                ("prime_group", ctypes.c_int32), ("grid", ctypes.c_int32), ("pipe_min_log_n", ctypes.c_int32),
+                ("launches", ctypes.c_int32),
                 ("device_bytes", ctypes.c_uint64), ("tuned_us", ctypes.c_double)]
 
 
@@ -95,7 +96,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "fpm_batch_run_device": ([vp, vp], ctypes.c_int),
         "fpm_batch_run": ([vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp)], ctypes.c_int),
         "fpm_batch_tune": ([vp, ctypes.c_int, ctypes.POINTER(FpmBatchInfo)], ctypes.c_int),
-        "fpm_batch_set_schedule": ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "fpm_batch_set_schedule": ([vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int],
+                                   ctypes.c_int),
         "fpm_batch_get_info": ([vp, ctypes.POINTER(FpmBatchInfo)], ctypes.c_int),
         "fpm_batch_free": ([vp], None),
         "fpm_server_create": ([ctypes.POINTER(vp), ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int, ctypes.c_int,
@@ -271,8 +273,9 @@ class Batch:
         _check(self._lib.fpm_batch_tune(self._h, reps, ctypes.byref(out)))
         return out
 
-    def set_schedule(self, layout: int = 1, order: int = 1, prime_group: int = 0, grid: int = 0):
-        _check(self._lib.fpm_batch_set_schedule(self._h, layout, order, prime_group, grid))
+    def set_schedule(self, layout: int = 1, order: int = 1, prime_group: int = 0, grid: int = 0,
+                     pipe_min_log_n: int = 0):
+        _check(self._lib.fpm_batch_set_schedule(self._h, layout, order, prime_group, grid, pipe_min_log_n))
 
 
 class Server:

@@ -145,6 +145,8 @@ typedef struct fpm_batch_info {
     int32_t order;         /* 0 as given; 1 largest product first */
     int32_t prime_group;   /* primes per transform work item (0: all of a product's) */
     int32_t grid;          /* transform grids: 0 one block per tile, k > 0 persistent */
+    int32_t pipe_min_log_n; /* products with logN >= this (0: none) take the one-product
+                               pipelined decompose and CRT */
     int32_t launches;      /* kernel launches in one graph replay */
     uint64_t device_bytes; /* device memory the batch holds */
     double tuned_us;       /* graph time of the chosen schedule (0 until fpm_batch_tune) */
@@ -167,7 +169,8 @@ FPM_API int fpm_batch_run(fpm_batch* batch, const uint32_t* const* a, const uint
  * fastest; the result is reported in info (may be NULL). */
 FPM_API int fpm_batch_tune(fpm_batch* batch, int reps, fpm_batch_info* info);
 /* Sets a schedule explicitly (fields as in fpm_batch_info) and recaptures. */
-FPM_API int fpm_batch_set_schedule(fpm_batch* batch, int layout, int order, int prime_group, int grid);
+FPM_API int fpm_batch_set_schedule(fpm_batch* batch, int layout, int order, int prime_group, int grid,
+                                   int pipe_min_log_n);
 FPM_API int fpm_batch_get_info(const fpm_batch* batch, fpm_batch_info* out);
 FPM_API void fpm_batch_free(fpm_batch* batch);
 

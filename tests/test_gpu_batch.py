@@ -20,7 +20,9 @@ pytestmark = pytest.mark.gpu
 MIXED = [(65536, 2048, 0), (32768, 868, 0), (16384, 512, 0), (8192, 1747, 0), (4096, 128, 0), (2048, 256, 0),
          (1024, 64, 0), (64, 32, 0), (4096, 32, 0), (16384, 868, 31), (4096, 256, 31)]
 
-SCHEDULES = [(0, 1, 0, 0), (1, 1, 0, 0), (2, 1, 0, 0), (1, 0, 16, 1), (2, 1, 16, 2), (0, 0, 8, 1), (1, 1, 3, 0)]
+# (layout, order, prime_group, grid, pipe_min_log_n)
+SCHEDULES = [(0, 1, 0, 0, 0), (1, 1, 0, 0, 0), (2, 1, 0, 0, 0), (1, 0, 16, 1, 0), (2, 1, 16, 2, 0), (0, 0, 8, 1, 0),
+             (1, 1, 3, 0, 0), (1, 1, 0, 0, 11), (2, 0, 16, 1, 12), (0, 1, 0, 0, 16)]
 
 
 @pytest.fixture(scope="module")
@@ -58,13 +60,13 @@ def oracle_q(ctx):
     raise KeyError
 
 
-@pytest.mark.parametrize("sched", SCHEDULES, ids=lambda s: "L%d-o%d-g%d-p%d" % s)
+@pytest.mark.parametrize("sched", SCHEDULES, ids=lambda s: "L%d-o%d-g%d-p%d-pipe%d" % s)
 def test_batch_matches_plain(mixed, sched):
     ctxs, ops, expect = mixed
     with polymul.Batch(ctxs) as bt:
         bt.set_schedule(*sched)
         info = bt.info
-        assert (info.layout, info.order, info.prime_group, info.grid) == sched
+        assert (info.layout, info.order, info.prime_group, info.grid, info.pipe_min_log_n) == sched
         assert info.count == len(ctxs) and info.launches > 0
         for rep in range(2):   # a replay of the same graph gives the same results
             got = bt.run([a for a, _ in ops], [b for _, b in ops])
@@ -96,7 +98,7 @@ def test_batch_beyond_one_table(cuda):
             ops.append((a, b))
             expect.append(ctx.run(a, b))
         with polymul.Batch(ctxs) as bt:
-            for sched in [(0, 1, 0, 0), (1, 1, 4, 1)]:
+            for sched in [(0, 1, 0, 0, 0), (1, 1, 4, 1, 12)]:
                 bt.set_schedule(*sched)
                 got = bt.run([a for a, _ in ops], [b for _, b in ops])
                 for g, e in zip(got, expect):
@@ -129,6 +131,8 @@ def test_batch_errors(cuda):
         with polymul.Batch([ctx]) as bt:
             with pytest.raises(polymul.FpmError) as e:
                 bt.set_schedule(3, 1, 0, 0)
+            with pytest.raises(polymul.FpmError):
+                bt.set_schedule(1, 1, 0, 0, 40)
             assert e.value.code == polymul.FPM_EINVAL
             with pytest.raises(polymul.FpmError):
                 bt.buffers(1)
