@@ -5,11 +5,14 @@
 // Reference counterparts (Akram275/fherma-polymult): k_ntt_cols solve.cu:130-166,
 // k_ntt_rows_mul solve.cu:195-233, with the stage structure of
 // rns_kernels.cuh:105-174.  Here (ntt_engine.cuh):
-//   * every pass keeps 8 elements per thread in registers for up to three
-//     stages at a time; the first and last rounds read and write global memory
-//     directly, shared memory carries only the exchanges between rounds;
-//   * A and B share each twiddle load, a round's 7 twiddles come in 3 vector
-//     loads;
+//   * the column passes keep 16 elements per thread in registers for up to
+//     four stages at a time where that saves a round (8 and three otherwise),
+//     the row pass 8 for up to three; the first and last rounds read and write
+//     global memory directly, shared memory carries only the exchanges between
+//     rounds;
+//   * A and B share each twiddle load, a round's 7 (15) twiddles come in 3 (8)
+//     vector loads; the row pass's generated tables are stored round-major, so
+//     those loads are free of bank conflicts;
 //   * the row pass builds only the FORWARD twiddle tables of its rows, from two
 //     small per-prime tables, and pairs row u with row R - 1 - u: the inverse
 //     twiddle of row u at entry y is minus the forward twiddle of row R - 1 - u
@@ -29,41 +32,45 @@ namespace fpm {
 
 namespace {
 
-template <int NSUB, int XS, class SWZ>
-using RP = Rounds<NSUB, XS, SWZ>;
+template <int NSUB, int XS, class SWZ, int RB>
+using RP = Rounds<NSUB, XS, SWZ, RB>;
+
+// Column-pass shared layout for RB register bits.
+template <int RB>
+using SwzC = std::conditional_t<RB == 3, SwzCol, SwzRow>;
 
 // Round R through shared memory on NV tiles.
-template <int NSUB, int XS, class SWZ, int R, bool LAZY, int NV, class TW>
+template <int NSUB, int XS, class SWZ, int RB, int R, bool LAZY, int NV, class TW>
 __device__ __forceinline__ void fwd_step(uint32_t* const (&tiles)[NV], const TW& tw, uint32_t p) {
-    const uint32_t base = round_base<NSUB, XS, SWZ, R>(threadIdx.x);
-    uint32_t v[NV][8];
+    const uint32_t base = round_base<NSUB, XS, SWZ, RB, R>(threadIdx.x);
+    uint32_t v[NV][1 << RB];
 #pragma unroll
-    for (int o = 0; o < NV; ++o) load_round<NSUB, XS, SWZ, R>(tiles[o], v[o], base);
-    fwd_round<NSUB, XS, SWZ, R, LAZY, NV>(v, base, tw, p);
+    for (int o = 0; o < NV; ++o) load_round<NSUB, XS, SWZ, RB, R>(tiles[o], v[o], base);
+    fwd_round<NSUB, XS, SWZ, RB, R, LAZY, NV>(v, base, tw, p);
 #pragma unroll
-    for (int o = 0; o < NV; ++o) store_round<NSUB, XS, SWZ, R>(tiles[o], v[o], base);
+    for (int o = 0; o < NV; ++o) store_round<NSUB, XS, SWZ, RB, R>(tiles[o], v[o], base);
     __syncthreads();
 }
 
-template <int NSUB, int XS, class SWZ, int R, int REND, bool LAZY, int NV, class TW>
+template <int NSUB, int XS, class SWZ, int RB, int R, int REND, bool LAZY, int NV, class TW>
 __device__ __forceinline__ void fwd_range(uint32_t* const (&tiles)[NV], const TW& tw, uint32_t p) {
     if constexpr (R < REND) {
-        fwd_step<NSUB, XS, SWZ, R, LAZY, NV>(tiles, tw, p);
-        fwd_range<NSUB, XS, SWZ, R + 1, REND, LAZY, NV>(tiles, tw, p);
+        fwd_step<NSUB, XS, SWZ, RB, R, LAZY, NV>(tiles, tw, p);
+        fwd_range<NSUB, XS, SWZ, RB, R + 1, REND, LAZY, NV>(tiles, tw, p);
     }
 }
 
 // Inverse rounds R, R - 1, ..., RLO through shared memory.
-template <int NSUB, int XS, class SWZ, int R, int RLO, bool LAZY, bool NEG, class TW>
+template <int NSUB, int XS, class SWZ, int RB, int R, int RLO, bool LAZY, bool NEG, class TW>
 __device__ __forceinline__ void inv_range(uint32_t* tile, const TW& tw, uint32_t p) {
     if constexpr (R >= RLO) {
-        const uint32_t base = round_base<NSUB, XS, SWZ, R>(threadIdx.x);
-        uint32_t v[8];
-        load_round<NSUB, XS, SWZ, R>(tile, v, base);
-        inv_round<NSUB, XS, SWZ, R, LAZY, NEG>(v, base, tw, p);
-        store_round<NSUB, XS, SWZ, R>(tile, v, base);
+        const uint32_t base = round_base<NSUB, XS, SWZ, RB, R>(threadIdx.x);
+        uint32_t v[1 << RB];
+        load_round<NSUB, XS, SWZ, RB, R>(tile, v, base);
+        inv_round<NSUB, XS, SWZ, RB, R, LAZY, NEG>(v, base, tw, p);
+        store_round<NSUB, XS, SWZ, RB, R>(tile, v, base);
         __syncthreads();
-        inv_range<NSUB, XS, SWZ, R - 1, RLO, LAZY, NEG>(tile, tw, p);
+        inv_range<NSUB, XS, SWZ, RB, R - 1, RLO, LAZY, NEG>(tile, tw, p);
     }
 }
 
@@ -84,26 +91,26 @@ __device__ __forceinline__ size_t col_offset(uint32_t i, uint32_t S, uint32_t c0
     return static_cast<size_t>(i >> XS) * S + c0 + (i & ((1u << XS) - 1u));
 }
 
-template <int LOGR, int R, int NV>
-__device__ __forceinline__ void col_global_load(const uint32_t* const (&X)[NV], uint32_t (&v)[NV][8], uint32_t base,
-                                                uint32_t S, uint32_t c0) {
-    constexpr int XS = 11 - LOGR, sh = RP<LOGR, XS, SwzCol>::lo(R);
+template <int LOGR, int RB, int R, int NV>
+__device__ __forceinline__ void col_global_load(const uint32_t* const (&X)[NV], uint32_t (&v)[NV][1 << RB],
+                                                uint32_t base, uint32_t S, uint32_t c0) {
+    constexpr int XS = 11 - LOGR, sh = RP<LOGR, XS, SwzC<RB>, RB>::lo(R);
     const size_t at = col_offset<LOGR>(base, S, c0);
     const size_t step = static_cast<size_t>(S) << sh;
 #pragma unroll
-    for (int k = 0; k < 8; ++k)
+    for (int k = 0; k < (1 << RB); ++k)
 #pragma unroll
         for (int o = 0; o < NV; ++o) v[o][k] = X[o][at + k * step];
 }
 
-template <int LOGR, int R, int NV>
-__device__ __forceinline__ void col_global_store(uint32_t* const (&X)[NV], const uint32_t (&v)[NV][8], uint32_t base,
-                                                 uint32_t S, uint32_t c0) {
-    constexpr int XS = 11 - LOGR, sh = RP<LOGR, XS, SwzCol>::lo(R);
+template <int LOGR, int RB, int R, int NV>
+__device__ __forceinline__ void col_global_store(uint32_t* const (&X)[NV], const uint32_t (&v)[NV][1 << RB],
+                                                 uint32_t base, uint32_t S, uint32_t c0) {
+    constexpr int XS = 11 - LOGR, sh = RP<LOGR, XS, SwzC<RB>, RB>::lo(R);
     const size_t at = col_offset<LOGR>(base, S, c0);
     const size_t step = static_cast<size_t>(S) << sh;
 #pragma unroll
-    for (int k = 0; k < 8; ++k)
+    for (int k = 0; k < (1 << RB); ++k)
 #pragma unroll
         for (int o = 0; o < NV; ++o) X[o][at + k * step] = v[o][k];
 }
@@ -111,74 +118,80 @@ __device__ __forceinline__ void col_global_store(uint32_t* const (&X)[NV], const
 template <int LOGR, bool LAZY>
 __device__ __forceinline__ void col_fwd_body(const DevPoint& d, uint32_t* A, uint32_t* B, int j, uint32_t bx) {
     extern __shared__ __align__(1024) uint32_t smem[];
+    constexpr int RB = col_pass_rb(LOGR), E = 1 << RB, T = ntt_threads<RB>();
     constexpr int XS = 11 - LOGR;
+    using SWZ = SwzC<RB>;
+    static_assert(RP<LOGR, XS, SWZ, RB>::all_conflict_free(), "column rounds must be free of bank conflicts");
     constexpr uint32_t R = 1u << LOGR, C = 1u << XS;
-    constexpr int last = RP<LOGR, XS, SwzCol>::kCount - 1;
+    constexpr int last = RP<LOGR, XS, SWZ, RB>::kCount - 1;
     uint32_t* ta = smem;
     uint32_t* tb = smem + 2048;
     uint2* tw = reinterpret_cast<uint2*>(smem + 4096);
     const uint32_t S = 1u << d.logS, c0 = bx * C;
     const uint32_t p = d.pc[j].p;
     uint32_t* const X[2] = {A + static_cast<size_t>(j) * d.N, B + static_cast<size_t>(j) * d.N};
-    for (uint32_t y = threadIdx.x; y < R; y += kNttThreads) tw[y] = d.col_f[static_cast<size_t>(j) * R + y];
+    for (uint32_t y = threadIdx.x; y < R; y += T) tw[y] = d.col_f[static_cast<size_t>(j) * R + y];
     const SharedTable table{tw};
     uint32_t* const tiles[2] = {ta, tb};
     {
-        const uint32_t base = round_base<LOGR, XS, SwzCol, 0>(threadIdx.x);
-        uint32_t v[2][8];
+        const uint32_t base = round_base<LOGR, XS, SWZ, RB, 0>(threadIdx.x);
+        uint32_t v[2][E];
         const uint32_t* const Xc[2] = {X[0], X[1]};
-        col_global_load<LOGR, 0, 2>(Xc, v, base, S, c0);
+        col_global_load<LOGR, RB, 0, 2>(Xc, v, base, S, c0);
         __syncthreads();   // the twiddle table
-        fwd_round<LOGR, XS, SwzCol, 0, LAZY, 2>(v, base, table, p);
+        fwd_round<LOGR, XS, SWZ, RB, 0, LAZY, 2>(v, base, table, p);
 #pragma unroll
-        for (int o = 0; o < 2; ++o) store_round<LOGR, XS, SwzCol, 0>(tiles[o], v[o], base);
+        for (int o = 0; o < 2; ++o) store_round<LOGR, XS, SWZ, RB, 0>(tiles[o], v[o], base);
         __syncthreads();
     }
-    fwd_range<LOGR, XS, SwzCol, 1, last, LAZY, 2>(tiles, table, p);
+    fwd_range<LOGR, XS, SWZ, RB, 1, last, LAZY, 2>(tiles, table, p);
     {
-        const uint32_t base = round_base<LOGR, XS, SwzCol, last>(threadIdx.x);
-        uint32_t v[2][8];
+        const uint32_t base = round_base<LOGR, XS, SWZ, RB, last>(threadIdx.x);
+        uint32_t v[2][E];
 #pragma unroll
-        for (int o = 0; o < 2; ++o) load_round<LOGR, XS, SwzCol, last>(tiles[o], v[o], base);
-        fwd_round<LOGR, XS, SwzCol, last, LAZY, 2>(v, base, table, p);
-        col_global_store<LOGR, last, 2>(X, v, base, S, c0);
+        for (int o = 0; o < 2; ++o) load_round<LOGR, XS, SWZ, RB, last>(tiles[o], v[o], base);
+        fwd_round<LOGR, XS, SWZ, RB, last, LAZY, 2>(v, base, table, p);
+        col_global_store<LOGR, RB, last, 2>(X, v, base, S, c0);
     }
 }
 
 template <int LOGR, bool LAZY>
 __device__ __forceinline__ void col_inv_body(const DevPoint& d, uint32_t* A, int j, uint32_t bx) {
     extern __shared__ __align__(1024) uint32_t smem[];
+    constexpr int RB = col_pass_rb(LOGR), E = 1 << RB, T = ntt_threads<RB>();
     constexpr int XS = 11 - LOGR;
+    using SWZ = SwzC<RB>;
+    static_assert(RP<LOGR, XS, SWZ, RB>::all_conflict_free(), "column rounds must be free of bank conflicts");
     constexpr uint32_t R = 1u << LOGR, C = 1u << XS;
-    constexpr int last = RP<LOGR, XS, SwzCol>::kCount - 1;
+    constexpr int last = RP<LOGR, XS, SWZ, RB>::kCount - 1;
     uint32_t* ta = smem;
     uint2* tw = reinterpret_cast<uint2*>(smem + 2048);
     const uint32_t S = 1u << d.logS, c0 = bx * C;
     const uint32_t p = d.pc[j].p;
     uint32_t* const X[1] = {A + static_cast<size_t>(j) * d.N};
-    for (uint32_t y = threadIdx.x; y < R; y += kNttThreads) tw[y] = d.col_i[static_cast<size_t>(j) * R + y];
+    for (uint32_t y = threadIdx.x; y < R; y += T) tw[y] = d.col_i[static_cast<size_t>(j) * R + y];
     const SharedTable table{tw};
     {
-        const uint32_t base = round_base<LOGR, XS, SwzCol, last>(threadIdx.x);
-        uint32_t v[1][8];
+        const uint32_t base = round_base<LOGR, XS, SWZ, RB, last>(threadIdx.x);
+        uint32_t v[1][E];
         const uint32_t* const Xc[1] = {X[0]};
-        col_global_load<LOGR, last, 1>(Xc, v, base, S, c0);
+        col_global_load<LOGR, RB, last, 1>(Xc, v, base, S, c0);
         __syncthreads();
-        inv_round<LOGR, XS, SwzCol, last, LAZY, false>(v[0], base, table, p);
-        store_round<LOGR, XS, SwzCol, last>(ta, v[0], base);
+        inv_round<LOGR, XS, SWZ, RB, last, LAZY, false>(v[0], base, table, p);
+        store_round<LOGR, XS, SWZ, RB, last>(ta, v[0], base);
         __syncthreads();
     }
-    inv_range<LOGR, XS, SwzCol, last - 1, 1, LAZY, false>(ta, table, p);
+    inv_range<LOGR, XS, SWZ, RB, last - 1, 1, LAZY, false>(ta, table, p);
     {
-        const uint32_t base = round_base<LOGR, XS, SwzCol, 0>(threadIdx.x);
-        uint32_t v[1][8];
-        load_round<LOGR, XS, SwzCol, 0>(ta, v[0], base);
-        inv_round<LOGR, XS, SwzCol, 0, LAZY, false>(v[0], base, table, p);
+        const uint32_t base = round_base<LOGR, XS, SWZ, RB, 0>(threadIdx.x);
+        uint32_t v[1][E];
+        load_round<LOGR, XS, SWZ, RB, 0>(ta, v[0], base);
+        inv_round<LOGR, XS, SWZ, RB, 0, LAZY, false>(v[0], base, table, p);
         if constexpr (LAZY) {
 #pragma unroll
-            for (int k = 0; k < 8; ++k) v[0][k] = reduce_once(v[0][k], p);   // y_j canonical for the CRT
+            for (int k = 0; k < E; ++k) v[0][k] = reduce_once(v[0][k], p);   // y_j canonical for the CRT
         }
-        col_global_store<LOGR, 0, 1>(X, v, base, S, c0);
+        col_global_store<LOGR, RB, 0, 1>(X, v, base, S, c0);
     }
 }
 
@@ -190,6 +203,9 @@ __device__ __forceinline__ void col_inv_body(const DevPoint& d, uint32_t* A, int
 //
 // Forward table of row u, entry y in [2^lev, 2^(lev+1)), stage b = LOGS-1-lev:
 // psi^(2^b (1 + 2 bitrev(u)) + 2^(b+1+logR) bitrev(y - 2^lev)) = U[u][b] Q[y].
+// Tables are round-major: position row_table_pos(y) holds entry y, and the
+// plan stores Q in the same order, so position p is U[u][b(p)] Q'[p] with the
+// level of p equal to that of y.
 
 template <int LOGS>
 struct RowGeom {
@@ -211,29 +227,34 @@ __device__ __forceinline__ uint32_t row_of_slot(uint32_t slot, uint32_t u0, uint
     }
 }
 
-template <int LOGS>
+template <int LOGS, int T>
 __device__ __forceinline__ void row_tables(uint2* tf, const DevPoint& d, int j, uint32_t u0) {
     using RG = RowGeom<LOGS>;
     const PrimeConsts pc = d.pc[j];
     const uint32_t R = 1u << d.logR;
     const uint2* qf = d.row_q_f + static_cast<size_t>(j) * RG::S;
-    constexpr uint32_t kPer = RG::kSlots * RG::S / kNttThreads;   // 8, or 16 when G = 1
-    // Every generator load first, then the arithmetic (the loads are independent).
-    uint2 f[kPer], q1[kPer];
+    constexpr uint32_t kPer = RG::kSlots * RG::S / T;   // entries per thread: 8, 16 or 32
+    constexpr uint32_t kBatch = kPer < 8 ? kPer : 8;
 #pragma unroll
-    for (uint32_t t = 0; t < kPer; ++t) {
-        const uint32_t i = threadIdx.x + t * kNttThreads;
-        const uint32_t slot = i >> LOGS, y = i & (RG::S - 1);
-        const uint32_t u = row_of_slot<LOGS>(slot, u0, R);
-        const uint32_t b = y ? LOGS - 1 - (31 - __clz(y)) : 0;
-        f[t] = __ldg(d.row_u_f + (static_cast<size_t>(j) * R + u) * LOGS + b);
-        q1[t] = __ldg(qf + y);
-    }
+    for (uint32_t t0 = 0; t0 < kPer; t0 += kBatch) {
+        // A batch's generator loads first, then its arithmetic (the loads are
+        // independent).
+        uint2 f[kBatch], q1[kBatch];
 #pragma unroll
-    for (uint32_t t = 0; t < kPer; ++t) {
-        const uint32_t i = threadIdx.x + t * kNttThreads;
-        const uint32_t slot = i >> LOGS, y = i & (RG::S - 1);
-        if (y) tf[slot * RG::kStride + y] = make_twiddle(shoup(f[t].x, q1[t].x, q1[t].y, pc.p), pc);
+        for (uint32_t t = 0; t < kBatch; ++t) {
+            const uint32_t i = threadIdx.x + (t0 + t) * T;
+            const uint32_t slot = i >> LOGS, y = i & (RG::S - 1);
+            const uint32_t u = row_of_slot<LOGS>(slot, u0, R);
+            const uint32_t b = y ? LOGS - 1 - (31 - __clz(y)) : 0;
+            f[t] = __ldg(d.row_u_f + (static_cast<size_t>(j) * R + u) * LOGS + b);
+            q1[t] = __ldg(qf + y);
+        }
+#pragma unroll
+        for (uint32_t t = 0; t < kBatch; ++t) {
+            const uint32_t i = threadIdx.x + (t0 + t) * T;
+            const uint32_t slot = i >> LOGS, y = i & (RG::S - 1);
+            if (y) tf[slot * RG::kStride + y] = make_twiddle(shoup(f[t].x, q1[t].x, q1[t].y, pc.p), pc);
+        }
     }
 }
 
@@ -246,7 +267,9 @@ template <int LOGS, bool LAZY>
 __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, int j, uint32_t bx) {
     extern __shared__ __align__(1024) uint32_t smem[];
     using RG = RowGeom<LOGS>;
-    using RPR = RP<LOGS, 0, SwzRow>;
+    constexpr int RB = row_pass_rb(LOGS), E = 1 << RB, T = ntt_threads<RB>();
+    using RPR = RP<LOGS, 0, SwzRow, RB>;
+    static_assert(RPR::all_conflict_free(), "row rounds must be free of bank conflicts");
     constexpr int last = RPR::kCount - 1;
     uint32_t* ta = smem;
     uint32_t* tb = smem + 2048;
@@ -261,45 +284,45 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
     const RowTable<LOGS, RG::kStride, true, RG::kFlip> iw{tf};
     uint32_t* const tiles[2] = {ta, tb};
 
-    // Round 0 straight from global memory (the thread's 8 elements lie in one row).
+    // Round 0 straight from global memory (the thread's E elements lie in one row).
     {
-        const uint32_t base = round_base<LOGS, 0, SwzRow, 0>(threadIdx.x);
+        const uint32_t base = round_base<LOGS, 0, SwzRow, RB, 0>(threadIdx.x);
         constexpr int sh = RPR::lo(0);
         const size_t at = row_offset<LOGS>(base, u0, R);
-        uint32_t v[2][8];
+        uint32_t v[2][E];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
+        for (int k = 0; k < E; ++k) {
             v[0][k] = a[at + (k << sh)];
             v[1][k] = b[at + (k << sh)];
         }
-        row_tables<LOGS>(tf, d, j, u0);
+        row_tables<LOGS, T>(tf, d, j, u0);
         __syncthreads();
-        fwd_round<LOGS, 0, SwzRow, 0, LAZY, 2>(v, base, fw, p);
+        fwd_round<LOGS, 0, SwzRow, RB, 0, LAZY, 2>(v, base, fw, p);
 #pragma unroll
-        for (int o = 0; o < 2; ++o) store_round<LOGS, 0, SwzRow, 0>(tiles[o], v[o], base);
+        for (int o = 0; o < 2; ++o) store_round<LOGS, 0, SwzRow, RB, 0>(tiles[o], v[o], base);
         __syncthreads();
     }
-    fwd_range<LOGS, 0, SwzRow, 1, last, LAZY, 2>(tiles, fw, p);
+    fwd_range<LOGS, 0, SwzRow, RB, 1, last, LAZY, 2>(tiles, fw, p);
     // Last forward round, the pointwise product and the first inverse round in
     // registers.
     {
-        const uint32_t base = round_base<LOGS, 0, SwzRow, last>(threadIdx.x);
-        uint32_t v[2][8];
-        load_round<LOGS, 0, SwzRow, last>(ta, v[0], base);
-        load_round<LOGS, 0, SwzRow, last>(tb, v[1], base);
-        fwd_round<LOGS, 0, SwzRow, last, LAZY, 2>(v, base, fw, p);
+        const uint32_t base = round_base<LOGS, 0, SwzRow, RB, last>(threadIdx.x);
+        uint32_t v[2][E];
+        load_round<LOGS, 0, SwzRow, RB, last>(ta, v[0], base);
+        load_round<LOGS, 0, SwzRow, RB, last>(tb, v[1], base);
+        fwd_round<LOGS, 0, SwzRow, RB, last, LAZY, 2>(v, base, fw, p);
         if (mode == kRowForward) {
             if constexpr (LAZY) {
 #pragma unroll
-                for (int k = 0; k < 8; ++k) {
+                for (int k = 0; k < E; ++k) {
                     v[0][k] = canon4(v[0][k], p);
                     v[1][k] = canon4(v[1][k], p);
                 }
             }
-            store_round<LOGS, 0, SwzRow, last>(ta, v[0], base);
-            store_round<LOGS, 0, SwzRow, last>(tb, v[1], base);
+            store_round<LOGS, 0, SwzRow, RB, last>(ta, v[0], base);
+            store_round<LOGS, 0, SwzRow, RB, last>(tb, v[1], base);
             __syncthreads();
-            for (uint32_t i = threadIdx.x; i < 2048; i += kNttThreads) {
+            for (uint32_t i = threadIdx.x; i < 2048; i += T) {
                 const size_t at = row_offset<LOGS>(i, u0, R);
                 a[at] = ta[SwzRow::f(i)];
                 b[at] = tb[SwzRow::f(i)];
@@ -307,7 +330,7 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
             return;
         }
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
+        for (int k = 0; k < E; ++k) {
             uint32_t x = v[0][k], y = v[1][k];
             if constexpr (LAZY) {
                 // below 2p each, so the Montgomery product stays below 2p
@@ -316,27 +339,44 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
             }
             v[0][k] = mont_mul(x, y, p, pc.pneg);
         }
-        inv_round<LOGS, 0, SwzRow, last, LAZY, true>(v[0], base, iw, p);
-        store_round<LOGS, 0, SwzRow, last>(ta, v[0], base);
+        inv_round<LOGS, 0, SwzRow, RB, last, LAZY, true>(v[0], base, iw, p);
+        store_round<LOGS, 0, SwzRow, RB, last>(ta, v[0], base);
         __syncthreads();
     }
-    inv_range<LOGS, 0, SwzRow, last - 1, 1, LAZY, true>(ta, iw, p);
+    inv_range<LOGS, 0, SwzRow, RB, last - 1, 1, LAZY, true>(ta, iw, p);
     // Inverse round 0 straight to global memory.
     {
-        const uint32_t base = round_base<LOGS, 0, SwzRow, 0>(threadIdx.x);
+        const uint32_t base = round_base<LOGS, 0, SwzRow, RB, 0>(threadIdx.x);
         constexpr int sh = RPR::lo(0);
-        uint32_t v[8];
-        load_round<LOGS, 0, SwzRow, 0>(ta, v, base);
-        inv_round<LOGS, 0, SwzRow, 0, LAZY, true>(v, base, iw, p);
+        uint32_t v[E];
+        load_round<LOGS, 0, SwzRow, RB, 0>(ta, v, base);
+        inv_round<LOGS, 0, SwzRow, RB, 0, LAZY, true>(v, base, iw, p);
         if (LAZY && d.logR == 0) {
             // No column pass follows: these are the y_j, canonical for the CRT.
 #pragma unroll
-            for (int k = 0; k < 8; ++k) v[k] = reduce_once(v[k], p);
+            for (int k = 0; k < E; ++k) v[k] = reduce_once(v[k], p);
         }
         const size_t at = row_offset<LOGS>(base, u0, R);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) a[at + (k << sh)] = v[k];
+        for (int k = 0; k < E; ++k) a[at + (k << sh)] = v[k];
     }
+}
+
+// Threads of each pass, and the resident blocks per SM that the column
+// kernels' registers are sized for: 8-element rounds MIN8 blocks of 256
+// threads, 16-element rounds 8 blocks of 128 (64 registers, measured fastest
+// against 80 and 128).
+template <int LOGR>
+constexpr int col_threads() {
+    return ntt_threads<col_pass_rb(LOGR)>();
+}
+template <int LOGS>
+constexpr int row_threads() {
+    return ntt_threads<row_pass_rb(LOGS)>();
+}
+template <int LOGR, int MIN8>
+constexpr int col_min_blocks() {
+    return col_pass_rb(LOGR) == 3 ? MIN8 : 8;
 }
 
 // Blocks per prime of each pass.
@@ -353,21 +393,21 @@ __host__ __device__ __forceinline__ uint32_t row_blocks(uint32_t logR) {
 
 // Plain launches: grid (blocks per prime, K).
 template <int LOGR, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads) k_ntt_col_fwd(DevPoint d, uint32_t* A, uint32_t* B) {
+__global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>())) k_ntt_col_fwd(DevPoint d, uint32_t* A, uint32_t* B) {
     pdl_launch_dependents();
     pdl_wait();
     col_fwd_body<LOGR, LAZY>(d, A, B, blockIdx.y, blockIdx.x);
 }
 
 template <int LOGR, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads) k_ntt_col_inv(DevPoint d, uint32_t* A) {
+__global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>())) k_ntt_col_inv(DevPoint d, uint32_t* A) {
     pdl_launch_dependents();
     pdl_wait();
     col_inv_body<LOGR, LAZY>(d, A, blockIdx.y, blockIdx.x);
 }
 
 template <int LOGS, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads, 5) k_ntt_row(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
+__global__ void __launch_bounds__(row_threads<LOGS>(), 5) k_ntt_row(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
     pdl_launch_dependents();
     pdl_wait();
     row_body<LOGS, LAZY>(d, A, B, mode, blockIdx.y, blockIdx.x);
@@ -378,7 +418,7 @@ __global__ void __launch_bounds__(kNttThreads, 5) k_ntt_row(DevPoint d, uint32_t
 // j0 + local / per, tile local % per (an item is a group of one product's
 // primes).
 template <int LOGR, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads, 6) k_ntt_col_fwd_group(const __grid_constant__ GroupTable t) {
+__global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>())) k_ntt_col_fwd_group(const __grid_constant__ GroupTable t) {
     for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
         if (b != blockIdx.x) __syncthreads();   // the previous tile's shared memory
         const uint32_t i = group_locate(t, b);
@@ -389,7 +429,7 @@ __global__ void __launch_bounds__(kNttThreads, 6) k_ntt_col_fwd_group(const __gr
 }
 
 template <int LOGR, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads, 6) k_ntt_col_inv_group(const __grid_constant__ GroupTable t) {
+__global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>())) k_ntt_col_inv_group(const __grid_constant__ GroupTable t) {
     for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
         if (b != blockIdx.x) __syncthreads();
         const uint32_t i = group_locate(t, b);
@@ -400,7 +440,7 @@ __global__ void __launch_bounds__(kNttThreads, 6) k_ntt_col_inv_group(const __gr
 }
 
 template <int LOGS, bool LAZY>
-__global__ void __launch_bounds__(kNttThreads, 5) k_ntt_row_group(const __grid_constant__ GroupTable t) {
+__global__ void __launch_bounds__(row_threads<LOGS>(), 5) k_ntt_row_group(const __grid_constant__ GroupTable t) {
     for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
         if (b != blockIdx.x) __syncthreads();
         const uint32_t i = group_locate(t, b);
@@ -507,19 +547,28 @@ void with_log(uint32_t v, F&& f) {
 template <bool LAZY>
 void group_pass(const GroupTable* t, int pass, uint32_t logR, uint32_t logS, uint32_t grid, cudaStream_t st,
                 int* occupancy) {
-    auto run = [&](auto kernel, size_t smem) {
+    auto run = [&](auto kernel, int threads, size_t smem) {
         if (occupancy) {
-            check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kernel, kNttThreads, smem), "occupancy");
+            check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kernel, threads, smem), "occupancy");
         } else {
-            kernel<<<grid, kNttThreads, smem, st>>>(*t);
+            kernel<<<grid, threads, smem, st>>>(*t);
         }
     };
     if (pass == kPassColFwd) {
-        with_log(logR, [&](auto c) { run(k_ntt_col_fwd_group<decltype(c)::value, LAZY>, col_fwd_smem_t(c)); });
+        with_log(logR, [&](auto c) {
+            constexpr int L = decltype(c)::value;
+            run(k_ntt_col_fwd_group<L, LAZY>, col_threads<L>(), col_fwd_smem_t(L));
+        });
     } else if (pass == kPassColInv) {
-        with_log(logR, [&](auto c) { run(k_ntt_col_inv_group<decltype(c)::value, LAZY>, col_inv_smem_t(c)); });
+        with_log(logR, [&](auto c) {
+            constexpr int L = decltype(c)::value;
+            run(k_ntt_col_inv_group<L, LAZY>, col_threads<L>(), col_inv_smem_t(L));
+        });
     } else if (pass == kPassRow) {
-        with_log(logS, [&](auto c) { run(k_ntt_row_group<decltype(c)::value, LAZY>, row_smem_t<decltype(c)::value>()); });
+        with_log(logS, [&](auto c) {
+            constexpr int L = decltype(c)::value;
+            run(k_ntt_row_group<L, LAZY>, row_threads<L>(), row_smem_t<L>());
+        });
     } else {
         throw std::runtime_error("grouped transform: unknown pass");
     }
@@ -544,14 +593,14 @@ void attrs_all() {
 template <int LOGR, bool LAZY>
 void launch_col_fwd_t(const DevPoint& d, uint32_t* A, uint32_t* B, cudaStream_t st) {
     const dim3 grid((1u << d.logS) >> (11 - LOGR), d.K);
-    check(launch_pdl(k_ntt_col_fwd<LOGR, LAZY>, grid, dim3(kNttThreads), col_fwd_smem_t(LOGR), st, d, A, B),
+    check(launch_pdl(k_ntt_col_fwd<LOGR, LAZY>, grid, dim3(col_threads<LOGR>()), col_fwd_smem_t(LOGR), st, d, A, B),
           "col_fwd launch");
 }
 
 template <int LOGR, bool LAZY>
 void launch_col_inv_t(const DevPoint& d, uint32_t* A, cudaStream_t st) {
     const dim3 grid((1u << d.logS) >> (11 - LOGR), d.K);
-    check(launch_pdl(k_ntt_col_inv<LOGR, LAZY>, grid, dim3(kNttThreads), col_inv_smem_t(LOGR), st, d, A),
+    check(launch_pdl(k_ntt_col_inv<LOGR, LAZY>, grid, dim3(col_threads<LOGR>()), col_inv_smem_t(LOGR), st, d, A),
           "col_inv launch");
 }
 
@@ -560,7 +609,7 @@ void launch_row_t(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStr
     using RG = RowGeom<LOGS>;
     const uint32_t R = 1u << d.logR;
     const dim3 grid(RG::G >= 2 ? R / RG::G : R, d.K);
-    check(launch_pdl(k_ntt_row<LOGS, LAZY>, grid, dim3(kNttThreads), row_smem_t<LOGS>(), st, d, A, B, mode),
+    check(launch_pdl(k_ntt_row<LOGS, LAZY>, grid, dim3(row_threads<LOGS>()), row_smem_t<LOGS>(), st, d, A, B, mode),
           "row launch");
 }
 

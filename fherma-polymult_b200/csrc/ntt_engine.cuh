@@ -4,24 +4,30 @@
 // tile index i carries the position x inside a sub-transform in bits
 // [XS, XS + NSUB) and the sub-transform's id in the other bits (the row pass
 // keeps rows contiguous, XS = 0; the column pass keeps a row's C = 2^XS
-// columns contiguous, XS = 11 - NSUB).  256 threads each hold 8 elements in
-// registers per "round" and apply up to three radix-2 stages to them between
-// exchanges through shared memory.
+// columns contiguous, XS = 11 - NSUB).  2^(11 - RB) threads each hold E = 2^RB
+// elements in registers per "round" and apply up to RB radix-2 stages to them
+// between exchanges through shared memory (RB = 3: 256 threads x 8 elements;
+// RB = 4: 128 threads x 16 elements, half the exchanges for NSUB = 7, 8, 10, 11).
 //
-// Round r covers the stage bits [lo, lo + cnt) of x, lo = NSUB - 3r - cnt
-// (cnt = 3 but for a short last round); a thread's 8 elements differ in the x
-// bits lo, lo + 1, lo + 2, i.e. element k sits at base | (k << (XS + lo)).
+// Round r covers the stage bits [lo, lo + cnt) of x, lo = NSUB - RB r - cnt
+// (cnt = RB but for a short last round, which has lo = 0); a thread's E elements
+// differ in the x bits lo .. lo + RB - 1, i.e. element k sits at
+// base | (k << (XS + lo)).
 //
 // Shared memory is swizzled by a GF(2)-linear map of the word index (SWZ::f).
 // Within a round the 32 lanes of a warp take 5 "lane bits" chosen so that each
 // bank bit depends on exactly one lane bit; every shared access of a round is
-// then free of bank conflicts (for the sizes the engine is used at).
+// then free of bank conflicts.  Rounds<>::conflict_free() checks this at compile
+// time for every round a kernel instantiates.
 //
 // Twiddles: the forward stage of distance 2^s pairs x and x + 2^s and uses
 // entry 2^(NSUB-1-s) + (x >> (s+1)) of the sub-transform's table (the
 // reference's psi^bitrev(m + i), rns_kernels.cuh:132-157, restricted to one
-// sub-transform).  A round's (up to) 7 twiddles are entries y, 2y, 2y + 1 and
-// 4y .. 4y + 3 for one y, so they arrive in three vector loads.
+// sub-transform).  A round's twiddles are, for one y, the entries
+// (y << t) .. (y << t) + 2^t - 1 of each level t < RB (level t is the stage of
+// register bit RB - 1 - t): 1 + 2 + 4 (+ 8) entries in 16-byte vector loads.
+// The row pass stores its tables round-major (row_table_pos), so that the lanes
+// of a round, which may differ in y, read consecutive 16-byte pairs.
 //
 // Butterflies come in two forms (arith.cuh): LAZY (Harvey: values below 4p in
 // the forward direction and below 2p in the inverse, needs p < 2^30) and full
@@ -32,17 +38,25 @@
 
 namespace fpm {
 
-constexpr int kNttThreads = 256;
+// Threads of a transform block holding RB register bits per round.
+template <int RB>
+constexpr int ntt_threads() {
+    return 1 << (11 - RB);
+}
+constexpr int kNttThreads = ntt_threads<3>();
 
-// Row pass: bank bit c of word i is i_c ^ i_{c+5}.
+// Row-pass layout: bank bit c of word i is i_c ^ i_{c+5}.  Any window of four
+// contiguous register bits holds at most one of c, c + 5.
 struct SwzRow {
-    static __device__ __forceinline__ uint32_t f(uint32_t i) { return i ^ ((i >> 5) & 31u); }
+    static constexpr __host__ __device__ uint32_t f(uint32_t i) { return i ^ ((i >> 5) & 31u); }
     static constexpr __host__ __device__ int partner(int c) { return c + 5; }
 };
-// Column pass: the 128-byte TMA swizzle (16-byte chunk index ^= 128-byte line
-// index mod 8); bank bits 0, 1 are i_0, i_1 and bank bit c >= 2 is i_c ^ i_{c+3}.
+// Column layout for 8-element rounds: the 128-byte TMA swizzle (16-byte chunk
+// index ^= 128-byte line index mod 8); bank bits 0, 1 are i_0, i_1 and bank bit
+// c >= 2 is i_c ^ i_{c+3}.  (A 4-bit register window can hold c and c + 3, so
+// 16-element rounds use SwzRow.)
 struct SwzCol {
-    static __device__ __forceinline__ uint32_t f(uint32_t i) { return i ^ (((i >> 5) & 7u) << 2); }
+    static constexpr __host__ __device__ uint32_t f(uint32_t i) { return i ^ (((i >> 5) & 7u) << 2); }
     static constexpr __host__ __device__ int partner(int c) { return c >= 2 ? c + 3 : -1; }
 };
 
@@ -51,14 +65,17 @@ struct RoundMap {
     int warp[3];
 };
 
-template <int NSUB, int XS, class SWZ>
+template <int NSUB, int XS, class SWZ, int RB = 3>
 struct Rounds {
+    static_assert(RB == 3 || RB == 4, "8 or 16 elements per thread");
     static_assert(NSUB >= 6 && NSUB <= 11 && XS + NSUB <= 11, "2^6 .. 2^11-element sub-transforms");
-    static constexpr int kCount = (NSUB + 2) / 3;
-    static constexpr __host__ __device__ int cnt(int r) { return (r < kCount - 1 || NSUB % 3 == 0) ? 3 : NSUB % 3; }
-    static constexpr __host__ __device__ int lo(int r) { return NSUB - 3 * r - cnt(r); }
+    static constexpr int kRegs = 1 << RB;
+    static constexpr int kWarpBits = 6 - RB;
+    static constexpr int kCount = (NSUB + RB - 1) / RB;
+    static constexpr __host__ __device__ int cnt(int r) { return (r < kCount - 1 || NSUB % RB == 0) ? RB : NSUB % RB; }
+    static constexpr __host__ __device__ int lo(int r) { return NSUB - RB * r - cnt(r); }
     static constexpr __host__ __device__ bool is_reg(int r, int bit) {
-        return bit >= XS + lo(r) && bit < XS + lo(r) + 3;
+        return bit >= XS + lo(r) && bit < XS + lo(r) + RB;
     }
     static constexpr __host__ __device__ RoundMap map(int r) {
         RoundMap m{};
@@ -80,29 +97,88 @@ struct Rounds {
             m.lane[c] = pick;
             used[pick] = true;
         }
+        // Lanes in ascending bit order: any order keeps the exchanges free of
+        // conflicts, and this one gives the 8 lanes of a quarter-warp consecutive
+        // twiddle positions y where the round's lanes differ in y.
+        for (int a = 0; a < 5; ++a)
+            for (int c = 0; c + 1 < 5 - a; ++c)
+                if (m.lane[c] > m.lane[c + 1]) {
+                    const int s = m.lane[c];
+                    m.lane[c] = m.lane[c + 1];
+                    m.lane[c + 1] = s;
+                }
         int w = 0;
         for (int b = 0; b < 11; ++b)
             if (!used[b]) m.warp[w++] = b;
         return m;
     }
+    // The 32 lanes of a warp hit 32 distinct banks in every access of round r
+    // (the map is linear, so the warp bits and the register index only add a
+    // common offset).
+    static constexpr bool conflict_free(int r) {
+        const RoundMap m = map(r);
+        bool seen[32] = {};
+        for (uint32_t l = 0; l < 32; ++l) {
+            uint32_t i = 0;
+            for (int c = 0; c < 5; ++c) i |= ((l >> c) & 1u) << m.lane[c];
+            const uint32_t bank = SWZ::f(i) & 31u;
+            if (seen[bank]) return false;
+            seen[bank] = true;
+        }
+        return true;
+    }
+    static constexpr bool all_conflict_free() {
+        for (int r = 0; r < kCount; ++r)
+            if (!conflict_free(r)) return false;
+        return true;
+    }
 };
 
-// Bits of the lane (BITS = 5) or warp (BITS = 3) index that move by SH places.
-template <int NSUB, int XS, class SWZ, int R, bool LANE>
+// Register bits per round.  The column passes hold 16 elements per thread where
+// that saves a round (LOGR = 7, 8, 10, 11), else 8; the row pass, whose fused
+// product round keeps both operands' elements and two twiddle sets live, holds 8
+// (measured faster at every row length).
+constexpr __host__ __device__ int col_pass_rb(int log) { return (log + 3) / 4 < (log + 2) / 3 ? 4 : 3; }
+constexpr __host__ __device__ int row_pass_rb(int) { return 3; }
+
+// Twiddle-table layout of the row pass ("round-major").  Level l of a table
+// (entries [2^l, 2^(l+1)), the stage of distance 2^(NSUB-1-l)) is read in round
+// l / RB, whose twiddle position y lies in [2^LY, 2^(LY+1)), at local level
+// t = l - LY: entries (y << t) + i, i < 2^t.  For t >= 2 the pair {i, i + 1}
+// (i even) of y is stored at 2^l + 2 ((i / 2) 2^LY + y - 2^LY), so lanes that
+// differ in y read consecutive 16-byte pairs; levels with t < 2 keep entry order.
+constexpr __host__ __device__ int table_ly(int nsub, int rb, int l) {
+    const int r = l / rb, count = (nsub + rb - 1) / rb;
+    const int cnt = (r < count - 1 || nsub % rb == 0) ? rb : nsub % rb;
+    return rb * r + cnt - rb;
+}
+
+constexpr __host__ __device__ uint32_t row_table_pos(int nsub, int rb, uint32_t e) {
+    int l = 0;
+    while ((2u << l) <= e) ++l;
+    const int ly = table_ly(nsub, rb, l), t = l - ly;
+    if (t < 2) return e;
+    const uint32_t j = e - (1u << l), i = j & ((1u << t) - 1u), yo = j >> t;
+    return (1u << l) + (i & 1u) + 2u * (((i >> 1) << ly) + yo);
+}
+
+// Bits of the lane (5) or warp (kWarpBits) index that move by SH places.
+template <int NSUB, int XS, class SWZ, int RB, int R, bool LANE>
 __host__ __device__ constexpr uint32_t deposit_mask(int sh) {
-    constexpr RoundMap m = Rounds<NSUB, XS, SWZ>::map(R);
+    using RP = Rounds<NSUB, XS, SWZ, RB>;
+    constexpr RoundMap m = RP::map(R);
     uint32_t mask = 0;
-    for (int c = 0; c < (LANE ? 5 : 3); ++c)
+    for (int c = 0; c < (LANE ? 5 : RP::kWarpBits); ++c)
         if ((LANE ? m.lane[c] : m.warp[c]) - c == sh) mask |= 1u << c;
     return mask;
 }
 
-template <int NSUB, int XS, class SWZ, int R, bool LANE>
+template <int NSUB, int XS, class SWZ, int RB, int R, bool LANE>
 __device__ __forceinline__ uint32_t deposit(uint32_t x) {
     uint32_t b = 0;
 #pragma unroll
     for (int sh = 0; sh <= 10; ++sh) {
-        const uint32_t mask = deposit_mask<NSUB, XS, SWZ, R, LANE>(sh);
+        const uint32_t mask = deposit_mask<NSUB, XS, SWZ, RB, R, LANE>(sh);
         if (mask) b |= (x & mask) << sh;
     }
     return b;
@@ -110,25 +186,25 @@ __device__ __forceinline__ uint32_t deposit(uint32_t x) {
 
 // Logical index of element 0 of this thread in round R (lane bits and warp
 // bits deposited group-wise: bits that move by the same distance move together).
-template <int NSUB, int XS, class SWZ, int R>
+template <int NSUB, int XS, class SWZ, int RB, int R>
 __device__ __forceinline__ uint32_t round_base(uint32_t tid) {
-    return deposit<NSUB, XS, SWZ, R, true>(tid & 31u) | deposit<NSUB, XS, SWZ, R, false>(tid >> 5);
+    return deposit<NSUB, XS, SWZ, RB, R, true>(tid & 31u) | deposit<NSUB, XS, SWZ, RB, R, false>(tid >> 5);
 }
 
-template <int NSUB, int XS, class SWZ, int R>
-__device__ __forceinline__ void load_round(const uint32_t* tile, uint32_t (&v)[8], uint32_t base) {
-    constexpr int sh = XS + Rounds<NSUB, XS, SWZ>::lo(R);
+template <int NSUB, int XS, class SWZ, int RB, int R>
+__device__ __forceinline__ void load_round(const uint32_t* tile, uint32_t (&v)[1 << RB], uint32_t base) {
+    constexpr int sh = XS + Rounds<NSUB, XS, SWZ, RB>::lo(R);
     const uint32_t sb = SWZ::f(base);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = tile[sb ^ SWZ::f(static_cast<uint32_t>(k) << sh)];
+    for (int k = 0; k < (1 << RB); ++k) v[k] = tile[sb ^ SWZ::f(static_cast<uint32_t>(k) << sh)];
 }
 
-template <int NSUB, int XS, class SWZ, int R>
-__device__ __forceinline__ void store_round(uint32_t* tile, const uint32_t (&v)[8], uint32_t base) {
-    constexpr int sh = XS + Rounds<NSUB, XS, SWZ>::lo(R);
+template <int NSUB, int XS, class SWZ, int RB, int R>
+__device__ __forceinline__ void store_round(uint32_t* tile, const uint32_t (&v)[1 << RB], uint32_t base) {
+    constexpr int sh = XS + Rounds<NSUB, XS, SWZ, RB>::lo(R);
     const uint32_t sb = SWZ::f(base);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) tile[sb ^ SWZ::f(static_cast<uint32_t>(k) << sh)] = v[k];
+    for (int k = 0; k < (1 << RB); ++k) tile[sb ^ SWZ::f(static_cast<uint32_t>(k) << sh)] = v[k];
 }
 
 // ---- butterflies ------------------------------------------------------------------
@@ -165,56 +241,70 @@ __device__ __forceinline__ void bf_inv(uint32_t& x, uint32_t& y, uint2 w, uint32
     }
 }
 
-// ---- twiddle sources: entries y, {2y, 2y+1}, {4y .. 4y+3} of table g ---------------
+// ---- twiddle sources ---------------------------------------------------------------
 
-struct Tw7 {
-    uint2 w0, w1[2], w2[4];
+// A round's twiddles: level t (t < RB) holds 2^t entries at w[2^t - 1 ..].
+template <int RB>
+struct Tw {
+    uint2 w[(1 << RB) - 1];
 };
 
-struct SharedTable {    // one table for every sub-transform (16-byte aligned)
-    const uint2* t;
-    __device__ __forceinline__ Tw7 get(uint32_t, uint32_t y, int cnt) const {
-        Tw7 r;
-        if (cnt == 3) r.w0 = t[y];
-        if (cnt >= 2) {
-            const uint4 a = *reinterpret_cast<const uint4*>(t + 2 * y);
-            r.w1[0] = make_uint2(a.x, a.y);
-            r.w1[1] = make_uint2(a.z, a.w);
+// Entries (y << t) + i, i < 2^t, of table tb into r.w[2^t - 1 + i]; REV: into
+// r.w[2^t - 1 + (2^t - 1 - i)] (the reflected partner table reads backwards).
+// LY >= 0: the table is round-major (row_table_pos) and y lies in
+// [2^LY, 2^(LY+1)); LY < 0: entry order.
+template <int RB, int T, bool REV, int LY>
+__device__ __forceinline__ void tw_level(Tw<RB>& r, const uint2* tb, uint32_t y) {
+    constexpr int n = 1 << T, off = n - 1;
+    if constexpr (T == 0) {
+        r.w[0] = tb[y];
+    } else {
+#pragma unroll
+        for (int m = 0; m < n; m += 2) {
+            const uint32_t at = (LY >= 0 && T >= 2) ? ((1u << (LY + T)) + (static_cast<uint32_t>(m) << LY) +
+                                                       2u * (y - (1u << LY)))
+                                                    : (y << T) + m;
+            const uint4 a = *reinterpret_cast<const uint4*>(tb + at);
+            r.w[off + (REV ? n - 1 - m : m)] = make_uint2(a.x, a.y);
+            r.w[off + (REV ? n - 2 - m : m + 1)] = make_uint2(a.z, a.w);
         }
-        const uint4 b = *reinterpret_cast<const uint4*>(t + 4 * y);
-        const uint4 c = *reinterpret_cast<const uint4*>(t + 4 * y + 2);
-        r.w2[0] = make_uint2(b.x, b.y);
-        r.w2[1] = make_uint2(b.z, b.w);
-        r.w2[2] = make_uint2(c.x, c.y);
-        r.w2[3] = make_uint2(c.z, c.w);
+    }
+}
+
+// Levels RB - cnt .. RB - 1 (a short round skips its top levels).
+template <int RB, bool REV, int LY, int T = 0>
+__device__ __forceinline__ void tw_levels(Tw<RB>& r, const uint2* tb, uint32_t y, int cnt) {
+    if constexpr (T < RB) {
+        if (T >= RB - cnt) tw_level<RB, T, REV, LY>(r, tb, y);
+        tw_levels<RB, REV, LY, T + 1>(r, tb, y, cnt);
+    }
+}
+
+struct SharedTable {    // one table for every sub-transform, entry order (16-byte aligned)
+    const uint2* t;
+    template <int RB, int LY>
+    __device__ __forceinline__ Tw<RB> get(uint32_t, uint32_t y, int cnt) const {
+        Tw<RB> r;
+        tw_levels<RB, false, -1>(r, t, y, cnt);
         return r;
     }
 };
 
-// Table of sub-transform g at t + g * STRIDE entries.  REFLECT: read the
-// partner table (g ^ FLIP) at the index with its low bits complemented, which
-// holds the negated inverse twiddles (see ntt.cu); the vector order reverses.
+// Round-major table of sub-transform g at t + g * STRIDE entries.  REFLECT:
+// read the partner table (g ^ FLIP) at the position with its low bits
+// complemented, which holds the negated inverse twiddles (see ntt.cu); the
+// vector order reverses.
 template <int NSUB, int STRIDE, bool REFLECT, uint32_t FLIP>
 struct RowTable {
     const uint2* t;
-    __device__ __forceinline__ Tw7 get(uint32_t g, uint32_t y, int cnt) const {
+    template <int RB, int LY>
+    __device__ __forceinline__ Tw<RB> get(uint32_t g, uint32_t y, int cnt) const {
         const uint2* tb = t + (REFLECT ? (g ^ FLIP) : g) * STRIDE;
-        Tw7 r;
-        // y lies in [2^lev, 2^(lev+1)): its reflection is y ^ (2^lev - 1), and the
-        // children 2y + t, 4y + t reflect to 2y* + 1 - t, 4y* + 3 - t.
-        const uint32_t yy = REFLECT ? (y ^ ((1u << (31 - __clz(y))) - 1u)) : y;
-        if (cnt == 3) r.w0 = tb[yy];
-        if (cnt >= 2) {
-            const uint4 a = *reinterpret_cast<const uint4*>(tb + 2 * yy);
-            r.w1[REFLECT ? 1 : 0] = make_uint2(a.x, a.y);
-            r.w1[REFLECT ? 0 : 1] = make_uint2(a.z, a.w);
-        }
-        const uint4 b = *reinterpret_cast<const uint4*>(tb + 4 * yy);
-        const uint4 c = *reinterpret_cast<const uint4*>(tb + 4 * yy + 2);
-        r.w2[REFLECT ? 3 : 0] = make_uint2(b.x, b.y);
-        r.w2[REFLECT ? 2 : 1] = make_uint2(b.z, b.w);
-        r.w2[REFLECT ? 1 : 2] = make_uint2(c.x, c.y);
-        r.w2[REFLECT ? 0 : 3] = make_uint2(c.z, c.w);
+        // y lies in [2^LY, 2^(LY+1)): its reflection is y ^ (2^LY - 1), and the
+        // children (y << t) + i reflect to (y* << t) + 2^t - 1 - i.
+        const uint32_t yy = REFLECT ? (y ^ ((1u << LY) - 1u)) : y;
+        Tw<RB> r;
+        tw_levels<RB, REFLECT, LY>(r, tb, yy, cnt);
         return r;
     }
 };
@@ -222,60 +312,50 @@ struct RowTable {
 // ---- rounds --------------------------------------------------------------------------
 
 // Sub-transform id and the "virtual top" twiddle index y of the round.
-template <int NSUB, int XS, class SWZ, int R>
+template <int NSUB, int XS, class SWZ, int RB, int R>
 __device__ __forceinline__ void round_tw_pos(uint32_t base, uint32_t& g, uint32_t& y) {
-    constexpr int lo = Rounds<NSUB, XS, SWZ>::lo(R);
+    constexpr int lo = Rounds<NSUB, XS, SWZ, RB>::lo(R);
     const uint32_t x = (base >> XS) & ((1u << NSUB) - 1u);
     g = (base & ((1u << XS) - 1u)) | ((base >> (XS + NSUB)) << XS);
-    y = (1u << (NSUB - 3 - lo)) | (x >> (lo + 3));
+    y = (1u << (NSUB - RB - lo)) | (x >> (lo + RB));
 }
 
-// Forward stages of round R on NV operands sharing the twiddles.
-template <int NSUB, int XS, class SWZ, int R, bool LAZY, int NV, class TW>
-__device__ __forceinline__ void fwd_round(uint32_t (&v)[NV][8], uint32_t base, const TW& tw, uint32_t p) {
-    constexpr int cnt = Rounds<NSUB, XS, SWZ>::cnt(R);
+// Forward stages of round R on NV operands sharing the twiddles (distances
+// decreasing: level t works on register bit RB - 1 - t).
+template <int NSUB, int XS, class SWZ, int RB, int R, bool LAZY, int NV, class TW>
+__device__ __forceinline__ void fwd_round(uint32_t (&v)[NV][1 << RB], uint32_t base, const TW& tw, uint32_t p) {
+    constexpr int cnt = Rounds<NSUB, XS, SWZ, RB>::cnt(R);
     uint32_t g, y;
-    round_tw_pos<NSUB, XS, SWZ, R>(base, g, y);
-    const Tw7 w = tw.get(g, y, cnt);
-    if constexpr (cnt == 3) {
+    round_tw_pos<NSUB, XS, SWZ, RB, R>(base, g, y);
+    const Tw<RB> w = tw.template get<RB, NSUB - RB - Rounds<NSUB, XS, SWZ, RB>::lo(R)>(g, y, cnt);
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
+    for (int t = RB - cnt; t < RB; ++t) {
+        const int db = RB - 1 - t;
 #pragma unroll
-            for (int o = 0; o < NV; ++o) bf_fwd<LAZY>(v[o][k], v[o][k + 4], w.w0, p);
-    }
-    if constexpr (cnt >= 2) {
+        for (int k = 0; k < (1 << RB); ++k) {
+            if (k & (1 << db)) continue;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (k & 2) continue;
-#pragma unroll
-            for (int o = 0; o < NV; ++o) bf_fwd<LAZY>(v[o][k], v[o][k + 2], w.w1[k >> 2], p);
+            for (int o = 0; o < NV; ++o)
+                bf_fwd<LAZY>(v[o][k], v[o][k | (1 << db)], w.w[(1 << t) - 1 + (k >> (db + 1))], p);
         }
     }
-#pragma unroll
-    for (int k = 0; k < 8; k += 2)
-#pragma unroll
-        for (int o = 0; o < NV; ++o) bf_fwd<LAZY>(v[o][k], v[o][k + 1], w.w2[k >> 1], p);
 }
 
 // Inverse stages of round R (distances increasing).
-template <int NSUB, int XS, class SWZ, int R, bool LAZY, bool NEG, class TW>
-__device__ __forceinline__ void inv_round(uint32_t (&v)[8], uint32_t base, const TW& tw, uint32_t p) {
-    constexpr int cnt = Rounds<NSUB, XS, SWZ>::cnt(R);
+template <int NSUB, int XS, class SWZ, int RB, int R, bool LAZY, bool NEG, class TW>
+__device__ __forceinline__ void inv_round(uint32_t (&v)[1 << RB], uint32_t base, const TW& tw, uint32_t p) {
+    constexpr int cnt = Rounds<NSUB, XS, SWZ, RB>::cnt(R);
     uint32_t g, y;
-    round_tw_pos<NSUB, XS, SWZ, R>(base, g, y);
-    const Tw7 w = tw.get(g, y, cnt);
+    round_tw_pos<NSUB, XS, SWZ, RB, R>(base, g, y);
+    const Tw<RB> w = tw.template get<RB, NSUB - RB - Rounds<NSUB, XS, SWZ, RB>::lo(R)>(g, y, cnt);
 #pragma unroll
-    for (int k = 0; k < 8; k += 2) bf_inv<LAZY, NEG>(v[k], v[k + 1], w.w2[k >> 1], p);
-    if constexpr (cnt >= 2) {
+    for (int t = RB - 1; t >= RB - cnt; --t) {
+        const int db = RB - 1 - t;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (k & 2) continue;
-            bf_inv<LAZY, NEG>(v[k], v[k + 2], w.w1[k >> 2], p);
+        for (int k = 0; k < (1 << RB); ++k) {
+            if (k & (1 << db)) continue;
+            bf_inv<LAZY, NEG>(v[k], v[k | (1 << db)], w.w[(1 << t) - 1 + (k >> (db + 1))], p);
         }
-    }
-    if constexpr (cnt == 3) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) bf_inv<LAZY, NEG>(v[k], v[k + 4], w.w0, p);
     }
 }
 

@@ -1,6 +1,8 @@
 // Host-side setup tables for one point; see plan.h.
 #include "plan.h"
 
+#include "ntt_engine.cuh"
+
 #include <algorithm>
 #include <cmath>
 #include <stdexcept>
@@ -226,13 +228,16 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
                 pl.row_u_f[at] = pair(pow_mod(psi, e, p), p);
             }
         }
+        // Stored round-major (row_table_pos), the order the row pass reads.
+        const int rb = row_pass_rb(static_cast<int>(g.logS));
         for (uint32_t y = 1; y < S; ++y) {
             uint32_t lev = 0;   // y in [2^lev, 2^(lev+1)): stage b = logS - 1 - lev
             while ((2u << lev) <= y) ++lev;
             const uint32_t b = g.logS - 1 - lev;
             const uint32_t r = y - (1u << lev);
             const uint64_t e = (1ull << (b + 1 + g.logR)) * bitrev(r, lev);
-            pl.row_q_f[static_cast<size_t>(j) * S + y] = pair(pow_mod(psi, e, p), p);
+            const uint32_t at = row_table_pos(static_cast<int>(g.logS), rb, y);
+            pl.row_q_f[static_cast<size_t>(j) * S + at] = pair(pow_mod(psi, e, p), p);
         }
     }
 

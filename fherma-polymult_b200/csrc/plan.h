@@ -60,7 +60,8 @@ struct HostPlan {
     // for row u and group r' is psi^(2^b (1 + 2 bitrev_logR(u)) + 2^(b+1+logR) bitrev(r'))
     // = U[u][b] * Q[y] with y = 2^(logS-1-b) + r'.  (The inverse twiddles are
     // negated forward ones of the partner row R - 1 - u, see ntt.cu.)
-    //   row_u_f: K x R x logS pairs, row_q_f: K x S pairs (entry 0 unused).
+    //   row_u_f: K x R x logS pairs, row_q_f: K x S pairs (entry 0 unused), each
+    //   prime's S entries in the round-major order of row_table_pos.
     std::vector<uint2> row_u_f, row_q_f;
     // Small transforms (logN <= kSmallLogN): psi^bitrev_logN(y), K x N pairs.
     std::vector<uint2> full_f, full_i;
