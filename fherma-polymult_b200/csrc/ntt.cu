@@ -84,38 +84,44 @@ __device__ __forceinline__ uint32_t canon4(uint32_t x, uint32_t p) {
 // Column pass: a block owns C = 2^XS adjacent columns c0 .. c0 + C - 1 of one
 // prime and all R = 2^LOGR rows; tile index i = u C + c (row u = position in the
 // sub-transform, column c = sub-transform).  Element (u, c) is X[u S + c0 + c].
+// S = 2^LOGS is a template parameter too, so a thread's strided global
+// accesses are one base address plus immediates.
 
-template <int LOGR>
-__device__ __forceinline__ size_t col_offset(uint32_t i, uint32_t S, uint32_t c0) {
+template <int LOGR, int LOGS>
+__device__ __forceinline__ uint32_t col_offset(uint32_t i, uint32_t c0) {
     constexpr int XS = 11 - LOGR;
-    return static_cast<size_t>(i >> XS) * S + c0 + (i & ((1u << XS) - 1u));
+    return ((i >> XS) << LOGS) + c0 + (i & ((1u << XS) - 1u));
 }
 
-template <int LOGR, int RB, int R, int NV>
+template <int LOGR, int LOGS, int RB, int R, int NV>
 __device__ __forceinline__ void col_global_load(const uint32_t* const (&X)[NV], uint32_t (&v)[NV][1 << RB],
-                                                uint32_t base, uint32_t S, uint32_t c0) {
+                                                uint32_t base, uint32_t c0) {
     constexpr int XS = 11 - LOGR, sh = RP<LOGR, XS, SwzC<RB>, RB>::lo(R);
-    const size_t at = col_offset<LOGR>(base, S, c0);
-    const size_t step = static_cast<size_t>(S) << sh;
+    constexpr uint32_t step = (1u << LOGS) << sh;
+    const uint32_t at = col_offset<LOGR, LOGS>(base, c0);
 #pragma unroll
-    for (int k = 0; k < (1 << RB); ++k)
+    for (int o = 0; o < NV; ++o) {
+        const uint32_t* x = X[o] + at;
 #pragma unroll
-        for (int o = 0; o < NV; ++o) v[o][k] = X[o][at + k * step];
+        for (int k = 0; k < (1 << RB); ++k) v[o][k] = x[k * step];
+    }
 }
 
-template <int LOGR, int RB, int R, int NV>
+template <int LOGR, int LOGS, int RB, int R, int NV>
 __device__ __forceinline__ void col_global_store(uint32_t* const (&X)[NV], const uint32_t (&v)[NV][1 << RB],
-                                                 uint32_t base, uint32_t S, uint32_t c0) {
+                                                 uint32_t base, uint32_t c0) {
     constexpr int XS = 11 - LOGR, sh = RP<LOGR, XS, SwzC<RB>, RB>::lo(R);
-    const size_t at = col_offset<LOGR>(base, S, c0);
-    const size_t step = static_cast<size_t>(S) << sh;
+    constexpr uint32_t step = (1u << LOGS) << sh;
+    const uint32_t at = col_offset<LOGR, LOGS>(base, c0);
 #pragma unroll
-    for (int k = 0; k < (1 << RB); ++k)
+    for (int o = 0; o < NV; ++o) {
+        uint32_t* x = X[o] + at;
 #pragma unroll
-        for (int o = 0; o < NV; ++o) X[o][at + k * step] = v[o][k];
+        for (int k = 0; k < (1 << RB); ++k) x[k * step] = v[o][k];
+    }
 }
 
-template <int LOGR, bool LAZY>
+template <int LOGR, int LOGS, bool LAZY>
 __device__ __forceinline__ void col_fwd_body(const DevPoint& d, uint32_t* A, uint32_t* B, int j, uint32_t bx) {
     extern __shared__ __align__(1024) uint32_t smem[];
     constexpr int RB = col_pass_rb(LOGR), E = 1 << RB, T = ntt_threads<RB>();
@@ -127,9 +133,10 @@ __device__ __forceinline__ void col_fwd_body(const DevPoint& d, uint32_t* A, uin
     uint32_t* ta = smem;
     uint32_t* tb = smem + 2048;
     uint2* tw = reinterpret_cast<uint2*>(smem + 4096);
-    const uint32_t S = 1u << d.logS, c0 = bx * C;
+    constexpr size_t N = size_t(1) << (LOGR + LOGS);
+    const uint32_t c0 = bx * C;
     const uint32_t p = d.pc[j].p;
-    uint32_t* const X[2] = {A + static_cast<size_t>(j) * d.N, B + static_cast<size_t>(j) * d.N};
+    uint32_t* const X[2] = {A + j * N, B + j * N};
     for (uint32_t y = threadIdx.x; y < R; y += T) tw[y] = d.col_f[static_cast<size_t>(j) * R + y];
     const SharedTable table{tw};
     uint32_t* const tiles[2] = {ta, tb};
@@ -137,7 +144,7 @@ __device__ __forceinline__ void col_fwd_body(const DevPoint& d, uint32_t* A, uin
         const uint32_t base = round_base<LOGR, XS, SWZ, RB, 0>(threadIdx.x);
         uint32_t v[2][E];
         const uint32_t* const Xc[2] = {X[0], X[1]};
-        col_global_load<LOGR, RB, 0, 2>(Xc, v, base, S, c0);
+        col_global_load<LOGR, LOGS, RB, 0, 2>(Xc, v, base, c0);
         __syncthreads();   // the twiddle table
         fwd_round<LOGR, XS, SWZ, RB, 0, LAZY, 2>(v, base, table, p);
 #pragma unroll
@@ -151,11 +158,11 @@ __device__ __forceinline__ void col_fwd_body(const DevPoint& d, uint32_t* A, uin
 #pragma unroll
         for (int o = 0; o < 2; ++o) load_round<LOGR, XS, SWZ, RB, last>(tiles[o], v[o], base);
         fwd_round<LOGR, XS, SWZ, RB, last, LAZY, 2>(v, base, table, p);
-        col_global_store<LOGR, RB, last, 2>(X, v, base, S, c0);
+        col_global_store<LOGR, LOGS, RB, last, 2>(X, v, base, c0);
     }
 }
 
-template <int LOGR, bool LAZY>
+template <int LOGR, int LOGS, bool LAZY>
 __device__ __forceinline__ void col_inv_body(const DevPoint& d, uint32_t* A, int j, uint32_t bx) {
     extern __shared__ __align__(1024) uint32_t smem[];
     constexpr int RB = col_pass_rb(LOGR), E = 1 << RB, T = ntt_threads<RB>();
@@ -166,16 +173,17 @@ __device__ __forceinline__ void col_inv_body(const DevPoint& d, uint32_t* A, int
     constexpr int last = RP<LOGR, XS, SWZ, RB>::kCount - 1;
     uint32_t* ta = smem;
     uint2* tw = reinterpret_cast<uint2*>(smem + 2048);
-    const uint32_t S = 1u << d.logS, c0 = bx * C;
+    constexpr size_t N = size_t(1) << (LOGR + LOGS);
+    const uint32_t c0 = bx * C;
     const uint32_t p = d.pc[j].p;
-    uint32_t* const X[1] = {A + static_cast<size_t>(j) * d.N};
+    uint32_t* const X[1] = {A + j * N};
     for (uint32_t y = threadIdx.x; y < R; y += T) tw[y] = d.col_i[static_cast<size_t>(j) * R + y];
     const SharedTable table{tw};
     {
         const uint32_t base = round_base<LOGR, XS, SWZ, RB, last>(threadIdx.x);
         uint32_t v[1][E];
         const uint32_t* const Xc[1] = {X[0]};
-        col_global_load<LOGR, RB, last, 1>(Xc, v, base, S, c0);
+        col_global_load<LOGR, LOGS, RB, last, 1>(Xc, v, base, c0);
         __syncthreads();
         inv_round<LOGR, XS, SWZ, RB, last, LAZY, false>(v[0], base, table, p);
         store_round<LOGR, XS, SWZ, RB, last>(ta, v[0], base);
@@ -191,7 +199,7 @@ __device__ __forceinline__ void col_inv_body(const DevPoint& d, uint32_t* A, int
 #pragma unroll
             for (int k = 0; k < E; ++k) v[0][k] = reduce_once(v[0][k], p);   // y_j canonical for the CRT
         }
-        col_global_store<LOGR, RB, 0, 1>(X, v, base, S, c0);
+        col_global_store<LOGR, LOGS, RB, 0, 1>(X, v, base, c0);
     }
 }
 
@@ -381,7 +389,7 @@ constexpr int col_min_blocks() {
 
 // Blocks per prime of each pass.
 template <int LOGR>
-__host__ __device__ __forceinline__ uint32_t col_blocks(uint32_t logS) {
+__host__ __device__ constexpr uint32_t col_blocks(uint32_t logS) {
     return (1u << logS) >> (11 - LOGR);
 }
 
@@ -392,18 +400,20 @@ __host__ __device__ __forceinline__ uint32_t row_blocks(uint32_t logR) {
 }
 
 // Plain launches: grid (blocks per prime, K).
-template <int LOGR, bool LAZY>
-__global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>())) k_ntt_col_fwd(DevPoint d, uint32_t* A, uint32_t* B) {
+template <int LOGR, int LOGS, bool LAZY>
+__global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>()))
+    k_ntt_col_fwd(DevPoint d, uint32_t* A, uint32_t* B) {
     pdl_launch_dependents();
     pdl_wait();
-    col_fwd_body<LOGR, LAZY>(d, A, B, blockIdx.y, blockIdx.x);
+    col_fwd_body<LOGR, LOGS, LAZY>(d, A, B, blockIdx.y, blockIdx.x);
 }
 
-template <int LOGR, bool LAZY>
-__global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>())) k_ntt_col_inv(DevPoint d, uint32_t* A) {
+template <int LOGR, int LOGS, bool LAZY>
+__global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>()))
+    k_ntt_col_inv(DevPoint d, uint32_t* A) {
     pdl_launch_dependents();
     pdl_wait();
-    col_inv_body<LOGR, LAZY>(d, A, blockIdx.y, blockIdx.x);
+    col_inv_body<LOGR, LOGS, LAZY>(d, A, blockIdx.y, blockIdx.x);
 }
 
 template <int LOGS, bool LAZY>
@@ -417,25 +427,29 @@ __global__ void __launch_bounds__(row_threads<LOGS>(), 5) k_ntt_row(DevPoint d, 
 // persistent) 1-D grid walks the table's blocks; block b of item i is prime
 // j0 + local / per, tile local % per (an item is a group of one product's
 // primes).
-template <int LOGR, bool LAZY>
-__global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>())) k_ntt_col_fwd_group(const __grid_constant__ GroupTable t) {
+template <int LOGR, int LOGS, bool LAZY>
+__global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>()))
+    k_ntt_col_fwd_group(const __grid_constant__ GroupTable t) {
+    constexpr uint32_t per = col_blocks<LOGR>(LOGS);
     for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
         if (b != blockIdx.x) __syncthreads();   // the previous tile's shared memory
         const uint32_t i = group_locate(t, b);
         const GroupItem& it = t.item[i];
-        const uint32_t local = b - t.first[i], per = col_blocks<LOGR>(it.d.logS);
-        col_fwd_body<LOGR, LAZY>(it.d, it.A, it.B, it.j0 + local / per, local % per);
+        const uint32_t local = b - t.first[i];
+        col_fwd_body<LOGR, LOGS, LAZY>(it.d, it.A, it.B, it.j0 + local / per, local % per);
     }
 }
 
-template <int LOGR, bool LAZY>
-__global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>())) k_ntt_col_inv_group(const __grid_constant__ GroupTable t) {
+template <int LOGR, int LOGS, bool LAZY>
+__global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>()))
+    k_ntt_col_inv_group(const __grid_constant__ GroupTable t) {
+    constexpr uint32_t per = col_blocks<LOGR>(LOGS);
     for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
         if (b != blockIdx.x) __syncthreads();
         const uint32_t i = group_locate(t, b);
         const GroupItem& it = t.item[i];
-        const uint32_t local = b - t.first[i], per = col_blocks<LOGR>(it.d.logS);
-        col_inv_body<LOGR, LAZY>(it.d, it.A, it.j0 + local / per, local % per);
+        const uint32_t local = b - t.first[i];
+        col_inv_body<LOGR, LOGS, LAZY>(it.d, it.A, it.j0 + local / per, local % per);
     }
 }
 
@@ -506,16 +520,18 @@ constexpr size_t row_smem_t() {
     return 2 * 2048 * sizeof(uint32_t) + RowGeom<LOGS>::kSlots * RowGeom<LOGS>::kStride * sizeof(uint2);
 }
 
-template <int LOGR, bool LAZY>
+template <int LOGR, int LOGS, bool LAZY>
 void col_attrs() {
     const int fwd = static_cast<int>(col_fwd_smem_t(LOGR)), inv = static_cast<int>(col_inv_smem_t(LOGR));
-    check(cudaFuncSetAttribute(k_ntt_col_fwd<LOGR, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, fwd),
+    check(cudaFuncSetAttribute(k_ntt_col_fwd<LOGR, LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, fwd),
           "col smem");
-    check(cudaFuncSetAttribute(k_ntt_col_inv<LOGR, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, inv),
+    check(cudaFuncSetAttribute(k_ntt_col_inv<LOGR, LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, inv),
           "col smem");
-    check(cudaFuncSetAttribute(k_ntt_col_fwd_group<LOGR, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, fwd),
+    check(cudaFuncSetAttribute(k_ntt_col_fwd_group<LOGR, LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               fwd),
           "col smem");
-    check(cudaFuncSetAttribute(k_ntt_col_inv_group<LOGR, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, inv),
+    check(cudaFuncSetAttribute(k_ntt_col_inv_group<LOGR, LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               inv),
           "col smem");
 }
 
@@ -542,6 +558,20 @@ void with_log(uint32_t v, F&& f) {
     }
 }
 
+// Calls f(integral_constant LOGR, integral_constant LOGS) for a four-step
+// geometry (make_geometry): LOGR = 6 with LOGS in [6, 11], or LOGS = 11 with
+// LOGR in [7, 11].
+template <class F>
+void with_cols(uint32_t logR, uint32_t logS, F&& f) {
+    if (logR == 6) {
+        with_log(logS, [&](auto s) { f(std::integral_constant<int, 6>{}, s); });
+    } else if (logS == 11) {
+        with_log(logR, [&](auto r) { f(r, std::integral_constant<int, 11>{}); });
+    } else {
+        throw std::runtime_error("unsupported transform geometry");
+    }
+}
+
 // One grouped pass: the kernel, its shared memory, and (occupancy) its
 // resident blocks per SM.
 template <bool LAZY>
@@ -555,14 +585,14 @@ void group_pass(const GroupTable* t, int pass, uint32_t logR, uint32_t logS, uin
         }
     };
     if (pass == kPassColFwd) {
-        with_log(logR, [&](auto c) {
-            constexpr int L = decltype(c)::value;
-            run(k_ntt_col_fwd_group<L, LAZY>, col_threads<L>(), col_fwd_smem_t(L));
+        with_cols(logR, logS, [&](auto r, auto s) {
+            constexpr int LR = decltype(r)::value, LS = decltype(s)::value;
+            run(k_ntt_col_fwd_group<LR, LS, LAZY>, col_threads<LR>(), col_fwd_smem_t(LR));
         });
     } else if (pass == kPassColInv) {
-        with_log(logR, [&](auto c) {
-            constexpr int L = decltype(c)::value;
-            run(k_ntt_col_inv_group<L, LAZY>, col_threads<L>(), col_inv_smem_t(L));
+        with_cols(logR, logS, [&](auto r, auto s) {
+            constexpr int LR = decltype(r)::value, LS = decltype(s)::value;
+            run(k_ntt_col_inv_group<LR, LS, LAZY>, col_threads<LR>(), col_inv_smem_t(LR));
         });
     } else if (pass == kPassRow) {
         with_log(logS, [&](auto c) {
@@ -576,12 +606,10 @@ void group_pass(const GroupTable* t, int pass, uint32_t logR, uint32_t logS, uin
 
 template <bool LAZY>
 void attrs_all() {
-    col_attrs<6, LAZY>();
-    col_attrs<7, LAZY>();
-    col_attrs<8, LAZY>();
-    col_attrs<9, LAZY>();
-    col_attrs<10, LAZY>();
-    col_attrs<11, LAZY>();
+    for (uint32_t s = 6; s <= 11; ++s)
+        with_cols(6, s, [&](auto lr, auto ls) { col_attrs<decltype(lr)::value, decltype(ls)::value, LAZY>(); });
+    for (uint32_t r = 7; r <= 11; ++r)
+        with_cols(r, 11, [&](auto lr, auto ls) { col_attrs<decltype(lr)::value, decltype(ls)::value, LAZY>(); });
     row_attrs<6, LAZY>();
     row_attrs<7, LAZY>();
     row_attrs<8, LAZY>();
@@ -590,18 +618,25 @@ void attrs_all() {
     row_attrs<11, LAZY>();
 }
 
-template <int LOGR, bool LAZY>
+template <bool LAZY>
 void launch_col_fwd_t(const DevPoint& d, uint32_t* A, uint32_t* B, cudaStream_t st) {
-    const dim3 grid((1u << d.logS) >> (11 - LOGR), d.K);
-    check(launch_pdl(k_ntt_col_fwd<LOGR, LAZY>, grid, dim3(col_threads<LOGR>()), col_fwd_smem_t(LOGR), st, d, A, B),
-          "col_fwd launch");
+    with_cols(d.logR, d.logS, [&](auto r, auto s) {
+        constexpr int LR = decltype(r)::value, LS = decltype(s)::value;
+        const dim3 grid(col_blocks<LR>(LS), d.K);
+        check(launch_pdl(k_ntt_col_fwd<LR, LS, LAZY>, grid, dim3(col_threads<LR>()), col_fwd_smem_t(LR), st, d, A,
+                         B),
+              "col_fwd launch");
+    });
 }
 
-template <int LOGR, bool LAZY>
+template <bool LAZY>
 void launch_col_inv_t(const DevPoint& d, uint32_t* A, cudaStream_t st) {
-    const dim3 grid((1u << d.logS) >> (11 - LOGR), d.K);
-    check(launch_pdl(k_ntt_col_inv<LOGR, LAZY>, grid, dim3(col_threads<LOGR>()), col_inv_smem_t(LOGR), st, d, A),
-          "col_inv launch");
+    with_cols(d.logR, d.logS, [&](auto r, auto s) {
+        constexpr int LR = decltype(r)::value, LS = decltype(s)::value;
+        const dim3 grid(col_blocks<LR>(LS), d.K);
+        check(launch_pdl(k_ntt_col_inv<LR, LS, LAZY>, grid, dim3(col_threads<LR>()), col_inv_smem_t(LR), st, d, A),
+              "col_inv launch");
+    });
 }
 
 template <int LOGS, bool LAZY>
@@ -619,16 +654,7 @@ void launch_ntt_t(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStr
     const bool row = mode == kRowProduct || mode == kRowForward || mode == kPassRow;
     const bool col_inv = mode == kRowProduct || mode == kPassColInv;
     const int row_mode = mode == kRowForward ? kRowForward : kRowProduct;
-    if (col_fwd) switch (d.logR) {
-        case 0: break;
-        case 6: launch_col_fwd_t<6, LAZY>(d, A, B, st); break;
-        case 7: launch_col_fwd_t<7, LAZY>(d, A, B, st); break;
-        case 8: launch_col_fwd_t<8, LAZY>(d, A, B, st); break;
-        case 9: launch_col_fwd_t<9, LAZY>(d, A, B, st); break;
-        case 10: launch_col_fwd_t<10, LAZY>(d, A, B, st); break;
-        case 11: launch_col_fwd_t<11, LAZY>(d, A, B, st); break;
-        default: throw std::runtime_error("unsupported column length");
-    }
+    if (col_fwd && d.logR) launch_col_fwd_t<LAZY>(d, A, B, st);
     if (row) switch (d.logS) {
         case 6: launch_row_t<6, LAZY>(d, A, B, row_mode, st); break;
         case 7: launch_row_t<7, LAZY>(d, A, B, row_mode, st); break;
@@ -638,16 +664,7 @@ void launch_ntt_t(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStr
         case 11: launch_row_t<11, LAZY>(d, A, B, row_mode, st); break;
         default: throw std::runtime_error("unsupported row length");
     }
-    if (col_inv) switch (d.logR) {
-        case 0: break;
-        case 6: launch_col_inv_t<6, LAZY>(d, A, st); break;
-        case 7: launch_col_inv_t<7, LAZY>(d, A, st); break;
-        case 8: launch_col_inv_t<8, LAZY>(d, A, st); break;
-        case 9: launch_col_inv_t<9, LAZY>(d, A, st); break;
-        case 10: launch_col_inv_t<10, LAZY>(d, A, st); break;
-        case 11: launch_col_inv_t<11, LAZY>(d, A, st); break;
-        default: throw std::runtime_error("unsupported column length");
-    }
+    if (col_inv && d.logR) launch_col_inv_t<LAZY>(d, A, st);
 }
 
 }  // namespace

@@ -87,7 +87,7 @@ Geometry make_geometry(uint32_t logN) {
         g.logS = logN;
         g.logR = 0;
     } else {
-        g.logS = (logN + 1) / 2;
+        g.logS = std::min<uint32_t>(kTileLog, logN - 6);
         g.logR = logN - g.logS;
     }
     return g;

@@ -62,8 +62,13 @@ def test_golden_vectors_reference_primes(cuda, entry):
         assert np.array_equal(ctx.run(g["a"], g["b"]), g["c"])
 
 
+# Every transform split: one block per prime (N <= 1024), the single row tile
+# (N = 2048), R = 64 columns with rows of 2^6 .. 2^11 (N = 2^12 .. 2^17), and
+# rows of 2048 with columns of 2^7 .. 2^11 (N = 2^18 .. 2^22, the 16-element
+# column rounds).
 GEOMETRIES = [(2, 33), (8, 97), (64, 100), (512, 250), (1024, 512), (2048, 129), (4096, 256), (8192, 868),
-              (16384, 300), (32768, 868), (65536, 2048), (1 << 17, 512)]
+              (16384, 300), (32768, 868), (65536, 2048), (1 << 17, 512), (1 << 18, 128), (1 << 19, 96),
+              (1 << 20, 64), (1 << 21, 48), (1 << 22, 32)]
 
 
 @pytest.mark.parametrize("prime_bits", [30, 31])
