@@ -20,6 +20,7 @@ struct DevPoint {
     const uint2* col_i;
     const uint2* row_u_f;      // K x R x logS
     const uint2* row_q_f;      // K x S
+    const uint2* row_tw;       // K x R x S: row u's forward table, round-major (built once)
     const uint2* full_f;       // K x N (small transforms)
     const uint2* full_i;
     const uint32_t* q;         // L

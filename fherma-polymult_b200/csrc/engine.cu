@@ -69,6 +69,7 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
         dp_.col_i = upload(pl.col_i);
         dp_.row_u_f = upload(pl.row_u_f);
         dp_.row_q_f = upload(pl.row_q_f);
+        dp_.row_tw = nullptr;
         dp_.lazy = pl.lazy ? 1 : 0;
         dp_.full_f = upload(pl.full_f);
         dp_.full_i = upload(pl.full_i);
@@ -93,6 +94,12 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
             const uint8_t* wa = upload(pl.dec_wimg_a);
             const uint8_t* wb = upload(pl.dec_wimg_b);
             dec_consts_.reset(new DecConsts(make_dec_consts(pl, wa, wb)));
+        }
+        if (!pl.g.small) {
+            uint2* tw = dalloc<uint2>(static_cast<size_t>(pl.K) * pl.N);
+            build_row_tables(dp_, tw, nullptr);
+            check(cudaDeviceSynchronize(), "row tables");
+            dp_.row_tw = tw;
         }
         dp_.err = dalloc<uint32_t>(1);
         check(cudaMemset(dp_.err, 0, sizeof(uint32_t)), "memset");

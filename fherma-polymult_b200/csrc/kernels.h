@@ -46,6 +46,9 @@ void launch_decompose(const DevPoint& d, const uint32_t* limbs, uint32_t* res, i
 // Residues A, B -> y_j in A (mode kRowProduct), or the forward transforms of
 // both in place (mode kRowForward).
 void launch_ntt(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStream_t st);
+// Every row's forward twiddle table (K x R x S, round-major) into out, from the
+// point's generators row_u_f and row_q_f; once per context.
+void build_row_tables(const DevPoint& d, uint2* out, cudaStream_t st);
 
 // The same on the tensor cores.
 void launch_decompose_tc(const DevPoint& d, const uint32_t* limbs, uint32_t* res, int operand, uint32_t n_begin,

@@ -74,6 +74,14 @@ __device__ __forceinline__ void inv_range(uint32_t* tile, const TW& tw, uint32_t
     }
 }
 
+// 16-byte asynchronous global -> shared copies (both addresses 16-byte aligned).
+__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Canonical residue from a lazy one (< 4p).
 __device__ __forceinline__ uint32_t canon4(uint32_t x, uint32_t p) {
     x = umin32(x, x - 2 * p);
@@ -213,7 +221,9 @@ __device__ __forceinline__ void col_inv_body(const DevPoint& d, uint32_t* A, int
 // psi^(2^b (1 + 2 bitrev(u)) + 2^(b+1+logR) bitrev(y - 2^lev)) = U[u][b] Q[y].
 // Tables are round-major: position row_table_pos(y) holds entry y, and the
 // plan stores Q in the same order, so position p is U[u][b(p)] Q'[p] with the
-// level of p equal to that of y.
+// level of p equal to that of y.  k_row_tables builds every row's table once
+// per context (K x R x S pairs); a row block copies its rows' tables into
+// shared memory asynchronously.
 
 template <int LOGS>
 struct RowGeom {
@@ -235,34 +245,44 @@ __device__ __forceinline__ uint32_t row_of_slot(uint32_t slot, uint32_t u0, uint
     }
 }
 
+// Copies the block's row tables (slot s holds row row_of_slot(s)) from the
+// prebuilt K x R x S array into shared memory with 16-byte asynchronous copies;
+// the caller waits with cp_async_wait_all() before its barrier.
 template <int LOGS, int T>
-__device__ __forceinline__ void row_tables(uint2* tf, const DevPoint& d, int j, uint32_t u0) {
+__device__ __forceinline__ void row_tables_async(uint2* tf, const DevPoint& d, int j, uint32_t u0) {
     using RG = RowGeom<LOGS>;
-    const PrimeConsts pc = d.pc[j];
     const uint32_t R = 1u << d.logR;
-    const uint2* qf = d.row_q_f + static_cast<size_t>(j) * RG::S;
-    constexpr uint32_t kPer = RG::kSlots * RG::S / T;   // entries per thread: 8, 16 or 32
-    constexpr uint32_t kBatch = kPer < 8 ? kPer : 8;
+    constexpr uint32_t kChunks = RG::kSlots * RG::S / 2;   // 16-byte pairs
+    static_assert(kChunks % T == 0, "whole chunks per thread");
 #pragma unroll
-    for (uint32_t t0 = 0; t0 < kPer; t0 += kBatch) {
-        // A batch's generator loads first, then its arithmetic (the loads are
-        // independent).
-        uint2 f[kBatch], q1[kBatch];
-#pragma unroll
-        for (uint32_t t = 0; t < kBatch; ++t) {
-            const uint32_t i = threadIdx.x + (t0 + t) * T;
-            const uint32_t slot = i >> LOGS, y = i & (RG::S - 1);
-            const uint32_t u = row_of_slot<LOGS>(slot, u0, R);
-            const uint32_t b = y ? LOGS - 1 - (31 - __clz(y)) : 0;
-            f[t] = __ldg(d.row_u_f + (static_cast<size_t>(j) * R + u) * LOGS + b);
-            q1[t] = __ldg(qf + y);
+    for (uint32_t t = 0; t < kChunks / T; ++t) {
+        const uint32_t c = threadIdx.x + t * T;
+        const uint32_t slot = c / (RG::S / 2), y = 2 * (c % (RG::S / 2));
+        const uint32_t u = row_of_slot<LOGS>(slot, u0, R);
+        const uint2* src = d.row_tw + (static_cast<size_t>(j) * R + u) * RG::S + y;
+        cp_async16(tf + slot * RG::kStride + y, src);
+    }
+    cp_async_commit();
+}
+
+// One row's forward table, position p (round-major): U[u][b(p)] Q'[p] with its
+// Shoup companion, where the plan stores Q' in the same order and b(p) =
+// LOGS - 1 - level(p).  Position 0 is unused.
+__global__ void __launch_bounds__(256) k_row_tables(DevPoint d, uint2* out) {
+    const int j = blockIdx.y;
+    const uint32_t u = blockIdx.x, logS = d.logS, S = 1u << logS, R = 1u << d.logR;
+    const PrimeConsts pc = d.pc[j];
+    const uint2* qf = d.row_q_f + static_cast<size_t>(j) * S;
+    const uint2* uf = d.row_u_f + (static_cast<size_t>(j) * R + u) * logS;
+    uint2* o = out + (static_cast<size_t>(j) * R + u) * S;
+    for (uint32_t p = threadIdx.x; p < S; p += blockDim.x) {
+        if (p == 0) {
+            o[0] = make_uint2(0, 0);
+            continue;
         }
-#pragma unroll
-        for (uint32_t t = 0; t < kBatch; ++t) {
-            const uint32_t i = threadIdx.x + (t0 + t) * T;
-            const uint32_t slot = i >> LOGS, y = i & (RG::S - 1);
-            if (y) tf[slot * RG::kStride + y] = make_twiddle(shoup(f[t].x, q1[t].x, q1[t].y, pc.p), pc);
-        }
+        const uint32_t b = logS - 1 - (31 - __clz(p));
+        const uint2 f = uf[b], q1 = qf[p];
+        o[p] = make_twiddle(shoup(f.x, q1.x, q1.y, pc.p), pc);
     }
 }
 
@@ -292,6 +312,8 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
     const RowTable<LOGS, RG::kStride, true, RG::kFlip> iw{tf};
     uint32_t* const tiles[2] = {ta, tb};
 
+    // The tables stream into shared memory while round 0 loads its elements.
+    row_tables_async<LOGS, T>(tf, d, j, u0);
     // Round 0 straight from global memory (the thread's E elements lie in one row).
     {
         const uint32_t base = round_base<LOGS, 0, SwzRow, RB, 0>(threadIdx.x);
@@ -303,7 +325,7 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
             v[0][k] = a[at + (k << sh)];
             v[1][k] = b[at + (k << sh)];
         }
-        row_tables<LOGS, T>(tf, d, j, u0);
+        cp_async_wait_all();
         __syncthreads();
         fwd_round<LOGS, 0, SwzRow, RB, 0, LAZY, 2>(v, base, fw, p);
 #pragma unroll
@@ -668,6 +690,11 @@ void launch_ntt_t(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStr
 }
 
 }  // namespace
+
+void build_row_tables(const DevPoint& d, uint2* out, cudaStream_t st) {
+    k_row_tables<<<dim3(1u << d.logR, d.K), 256, 0, st>>>(d, out);
+    check(cudaGetLastError(), "row tables launch");
+}
 
 void ntt_init_attributes() {
     attrs_all<true>();

@@ -101,6 +101,7 @@ size_t device_footprint(const HostPlan& pl) {
                bytes(pl.p_recip) + bytes(pl.dec_img_a) + bytes(pl.dec_img_b) + bytes(pl.dec_fold) +
                bytes(pl.dec_wimg_a) + bytes(pl.dec_wimg_b) +
                bytes(pl.crt_img) + bytes(pl.crt_img_v) + sizeof(uint32_t);
+    if (!pl.g.small) t += static_cast<size_t>(pl.K) * pl.N * sizeof(uint2);   // row twiddle tables
     t += 2 * static_cast<size_t>(pl.K) * pl.N * sizeof(uint32_t);   // residue workspaces
     t += 3 * static_cast<size_t>(pl.N) * pl.L * sizeof(uint32_t);   // host-path limb buffers
     return t;
