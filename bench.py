@@ -159,19 +159,20 @@ class ClockSampler:
 
 
 def algorithmic_bytes(N, L, K):
-    """Per product and per stage launch, from the six-pass RNS schedule with
-    twiddles cache-resident: decompose reads N L and writes K N words per
-    operand; the column pass reads and writes both operands' residues (4 K N);
-    the fused row pass reads 2 K N and writes K N; the inverse column pass reads
-    and writes K N each; the CRT reads K N and writes N L."""
+    """Per product and per stage launch, from the six-pass RNS schedule:
+    decompose reads N L and writes K N words per operand; the column pass reads
+    and writes both operands' residues (4 K N; its K x R twiddles stay in
+    cache); the fused row pass reads 2 K N and writes K N, and reads every
+    row's prebuilt twiddle table, K x N Shoup pairs (2 K N words); the inverse
+    column pass reads and writes K N each; the CRT reads K N and writes N L."""
     w = 4
     return {
         "decompose": w * (N * L + K * N),
         "ntt_col_fwd": w * 4 * K * N,
-        "ntt_row": w * 3 * K * N,
+        "ntt_row": w * 5 * K * N,
         "ntt_col_inv": w * 2 * K * N,
         "crt": w * (K * N + N * L),
-        "product": w * (3 * N * L + 12 * K * N),
+        "product": w * (3 * N * L + 14 * K * N),
     }
 
 
