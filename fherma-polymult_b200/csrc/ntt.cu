@@ -5,16 +5,16 @@
 // Reference counterparts (Akram275/fherma-polymult): k_ntt_cols solve.cu:130-166,
 // k_ntt_rows_mul solve.cu:195-233, with the stage structure of
 // rns_kernels.cuh:105-174.  Here (ntt_engine.cuh):
-//   * the column passes keep 16 elements per thread in registers for up to
-//     four stages at a time where that saves a round (8 and three otherwise),
-//     the row pass 8 for up to three; the first and last rounds read and write
-//     global memory directly, shared memory carries only the exchanges between
-//     rounds;
+//   * every pass keeps 16 elements per thread in registers for up to four
+//     stages at a time where that saves a round (8 and three otherwise); the
+//     first and last rounds read and write global memory directly, shared
+//     memory carries only the exchanges between rounds;
 //   * A and B share each twiddle load, a round's 7 (15) twiddles come in 3 (8)
-//     vector loads; the row pass's generated tables are stored round-major, so
-//     those loads are free of bank conflicts;
-//   * the row pass builds only the FORWARD twiddle tables of its rows, from two
-//     small per-prime tables, and pairs row u with row R - 1 - u: the inverse
+//     vector loads; the row pass's tables are stored round-major, so those
+//     loads are free of bank conflicts;
+//   * the row pass uses only the FORWARD twiddle tables of its rows (prebuilt
+//     once per context from two small per-prime tables), and pairs row u with
+//     row R - 1 - u: the inverse
 //     twiddle of row u at entry y is minus the forward twiddle of row R - 1 - u
 //     at y with its low bits complemented (psi^(N - e) = -psi^-e), so one
 //     table set serves both directions;
@@ -408,6 +408,12 @@ template <int LOGR, int MIN8>
 constexpr int col_min_blocks() {
     return col_pass_rb(LOGR) == 3 ? MIN8 : 8;
 }
+// Row kernels: five blocks of 256 threads (8-element rounds, 48 registers), or
+// six of 128 (16-element rounds, 80 registers: 64 spills).
+template <int LOGS>
+constexpr int row_min_blocks() {
+    return row_pass_rb(LOGS) == 3 ? 5 : 6;
+}
 
 // Blocks per prime of each pass.
 template <int LOGR>
@@ -439,7 +445,7 @@ __global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>(
 }
 
 template <int LOGS, bool LAZY>
-__global__ void __launch_bounds__(row_threads<LOGS>(), 5) k_ntt_row(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
+__global__ void __launch_bounds__(row_threads<LOGS>(), (row_min_blocks<LOGS>())) k_ntt_row(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
     pdl_launch_dependents();
     pdl_wait();
     row_body<LOGS, LAZY>(d, A, B, mode, blockIdx.y, blockIdx.x);
@@ -476,7 +482,7 @@ __global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>(
 }
 
 template <int LOGS, bool LAZY>
-__global__ void __launch_bounds__(row_threads<LOGS>(), 5) k_ntt_row_group(const __grid_constant__ GroupTable t) {
+__global__ void __launch_bounds__(row_threads<LOGS>(), (row_min_blocks<LOGS>())) k_ntt_row_group(const __grid_constant__ GroupTable t) {
     for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
         if (b != blockIdx.x) __syncthreads();
         const uint32_t i = group_locate(t, b);

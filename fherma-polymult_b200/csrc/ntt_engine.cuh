@@ -134,12 +134,12 @@ struct Rounds {
     }
 };
 
-// Register bits per round.  The column passes hold 16 elements per thread where
-// that saves a round (LOGR = 7, 8, 10, 11), else 8; the row pass, whose fused
-// product round keeps both operands' elements and two twiddle sets live, holds 8
-// (measured faster at every row length).
+// Register bits per round: every pass holds 16 elements per thread where that
+// saves a round (sub-transforms of 2^7, 2^8, 2^10, 2^11), else 8.  (The row pass
+// gains only since its twiddle tables are prebuilt: generating them in the
+// block cost twice as many entries per thread with 16-element rounds.)
 constexpr __host__ __device__ int col_pass_rb(int log) { return (log + 3) / 4 < (log + 2) / 3 ? 4 : 3; }
-constexpr __host__ __device__ int row_pass_rb(int) { return 3; }
+constexpr __host__ __device__ int row_pass_rb(int log) { return col_pass_rb(log); }
 
 // Twiddle-table layout of the row pass ("round-major").  Level l of a table
 // (entries [2^l, 2^(l+1)), the stage of distance 2^(NSUB-1-l)) is read in round
