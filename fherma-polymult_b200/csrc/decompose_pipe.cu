@@ -90,18 +90,19 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, vo
     return true;
 }
 
-// (lo + hi 2^32) mod p for the 49-bit sums: f = {p, 2^32 mod p, its Shoup
-// companion, floor(2^32 / p)}.  LAZY leaves a value below 4p, congruent to
-// the same residue, for a transform whose first butterflies take lazy input.
+// A GEMM sum D is below 4L 255^2 <= 256 * 65025 (L <= 64), so both halves of
+// sum_s D_s 2^(8s), A = D_0 + 2^8 D_1 and B = D_2 + 2^8 D_3, are below
+// 257 * 256 * 65025 < 2^32, and the residue is (A + B 2^16) mod p:
+// f = {p, 2^16 mod p, its Shoup companion, floor(2^32 / p)}.  LAZY leaves a
+// value below 4p, congruent to the same residue, for a transform whose first
+// butterflies take lazy input.
+static_assert(kMaxL <= 64, "D_0 + 2^8 D_1 must fit 32 bits");
 template <bool LAZY>
-__device__ __forceinline__ uint32_t fold49(uint64_t v, uint4 f) {
+__device__ __forceinline__ uint32_t fold_halves(uint32_t A, uint32_t B, uint4 f) {
     if constexpr (LAZY) {
-        return shoup_lazy(static_cast<uint32_t>(v), 1u, f.w, f.x) +
-               shoup_lazy(static_cast<uint32_t>(v >> 32), f.y, f.z, f.x);
+        return shoup_lazy(A, 1u, f.w, f.x) + shoup_lazy(B, f.y, f.z, f.x);
     } else {
-        const uint32_t lo = shoup(static_cast<uint32_t>(v), 1u, f.w, f.x);
-        const uint32_t hi = shoup(static_cast<uint32_t>(v >> 32), f.y, f.z, f.x);
-        return add_mod(lo, hi, f.x);
+        return add_mod(shoup(A, 1u, f.w, f.x), shoup(B, f.y, f.z, f.x), f.x);
     }
 }
 
@@ -277,9 +278,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                     for (int k = 0; k < 16; ++k) {
                         const int j = j0 + k;
                         const uint32_t* rr = r[k >> 3] + 4 * (k & 7);
-                        const uint64_t v = static_cast<uint64_t>(rr[0]) + (static_cast<uint64_t>(rr[1]) << 8) +
-                                           (static_cast<uint64_t>(rr[2]) << 16) + (static_cast<uint64_t>(rr[3]) << 24);
-                        if (live && j < K) res[static_cast<size_t>(j) * d.N + n0 + m] = fold49<LAZY>(v, fc.fold[j]);
+                        const uint32_t A = rr[0] + (rr[1] << 8), B = rr[2] + (rr[3] << 8);
+                        if (live && j < K) res[static_cast<size_t>(j) * d.N + n0 + m] = fold_halves<LAZY>(A, B, fc.fold[j]);
                     }
                 }
             }
@@ -300,7 +300,11 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 DecConsts make_dec_consts(const HostPlan& pl, const uint8_t* img_a, const uint8_t* img_b) {
     DecConsts dc{};
-    for (int j = 0; j < pl.K; ++j) dc.fold[j] = pl.dec_fold[j];
+    for (int j = 0; j < pl.K; ++j) {
+        const uint32_t p = pl.primes[j], r16 = (1u << 16) % p;
+        dc.fold[j] = uint4{p, r16, static_cast<uint32_t>((static_cast<uint64_t>(r16) << 32) / p),
+                           static_cast<uint32_t>((1ull << 32) / p)};
+    }
     dc.img[0] = img_a;
     dc.img[1] = img_b;
     dc.chunks = pl.dec_wchunks;

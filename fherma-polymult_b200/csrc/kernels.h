@@ -83,7 +83,7 @@ void launch_crt_pipe(const DevPoint& d, const CrtConsts& cc, const uint32_t* Y, 
 // b != nullptr the CTAs split between a -> A (operand 0) and b -> B (1),
 // otherwise all take a -> A as operand `operand0`.
 struct DecConsts {
-    uint4 fold[kMaxK];          // {p, 2^32 mod p, its Shoup companion, floor(2^32 / p)}
+    uint4 fold[kMaxK];          // {p, 2^16 mod p, its Shoup companion, floor(2^32 / p)}
     const uint8_t* img[2];      // device copies of the plan's wide images, operands a and b
     uint32_t chunks;            // chunks of 64 primes
     uint32_t last_cols;         // GEMM columns of the last chunk
