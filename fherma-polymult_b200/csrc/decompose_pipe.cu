@@ -300,11 +300,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
 DecConsts make_dec_consts(const HostPlan& pl, const uint8_t* img_a, const uint8_t* img_b) {
     DecConsts dc{};
-    for (int j = 0; j < pl.K; ++j) {
-        const uint32_t p = pl.primes[j], r16 = (1u << 16) % p;
-        dc.fold[j] = uint4{p, r16, static_cast<uint32_t>((static_cast<uint64_t>(r16) << 32) / p),
-                           static_cast<uint32_t>((1ull << 32) / p)};
-    }
+    for (int j = 0; j < pl.K; ++j) dc.fold[j] = pl.dec_fold[j];
     dc.img[0] = img_a;
     dc.img[1] = img_b;
     dc.chunks = pl.dec_wchunks;

@@ -63,12 +63,13 @@ __device__ inline Smem carve(uint8_t* base, uint32_t kb) {
     return s;
 }
 
-// (lo + hi 2^32) mod p for the 49-bit epilogue sums: f = {p, 2^32 mod p, its
-// Shoup companion, floor(2^32 / p)}.
-__device__ __forceinline__ uint32_t fold49(uint64_t v, uint4 f) {
-    const uint32_t lo = shoup(static_cast<uint32_t>(v), 1u, f.w, f.x);
-    const uint32_t hi = shoup(static_cast<uint32_t>(v >> 32), f.y, f.z, f.x);
-    return add_mod(lo, hi, f.x);
+// A GEMM sum D is below 4L 255^2 <= 256 * 65025 (L <= 64), so both halves of
+// sum_s D_s 2^(8s), A = D_0 + 2^8 D_1 and B = D_2 + 2^8 D_3, are below 2^32;
+// the residue is (A + B 2^16) mod p with f = {p, 2^16 mod p, its Shoup
+// companion, floor(2^32 / p)}.
+static_assert(kMaxL <= 64, "D_0 + 2^8 D_1 must fit 32 bits");
+__device__ __forceinline__ uint32_t fold_halves(uint32_t A, uint32_t B, uint4 f) {
+    return add_mod(shoup(A, 1u, f.w, f.x), shoup(B, f.y, f.z, f.x), f.x);
 }
 
 // Coefficients n0 .. n0 + nk - 1 (nk <= 128) of one operand.
@@ -215,10 +216,7 @@ __device__ __forceinline__ void dec_body(const DevPoint& d, const uint32_t* __re
                 uint32_t out[8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
-                    const uint64_t v = static_cast<uint64_t>(r[4 * i]) + (static_cast<uint64_t>(r[4 * i + 1]) << 8) +
-                                       (static_cast<uint64_t>(r[4 * i + 2]) << 16) +
-                                       (static_cast<uint64_t>(r[4 * i + 3]) << 24);
-                    out[i] = fold49(v, f[i]);
+                    out[i] = fold_halves(r[4 * i] + (r[4 * i + 1] << 8), r[4 * i + 2] + (r[4 * i + 3] << 8), f[i]);
                 }
                 if (m < nk) {
 #pragma unroll

@@ -258,8 +258,8 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
     pl.dec_wimg_b.assign(pl.dec_wimg_a.size(), 0);
     for (int j = 0; j < K; ++j) {
         const uint32_t p = pl.primes[j];
-        const uint32_t r32 = static_cast<uint32_t>((1ull << 32) % p);
-        pl.dec_fold[j] = uint4{p, r32, shoup_of(r32, p), static_cast<uint32_t>((1ull << 32) / p)};
+        const uint32_t r16 = (1u << 16) % p;
+        pl.dec_fold[j] = uint4{p, r16, shoup_of(r16, p), static_cast<uint32_t>((1ull << 32) / p)};
         const uint32_t scale_b = pl.dec_b[static_cast<size_t>(j) * L].x;   // 2^0 * scale
         const size_t chunk = static_cast<size_t>(j / 32) * dchunk;
         for (int s = 0; s < 4; ++s) {

@@ -88,7 +88,7 @@ struct HostPlan {
     // pipelined decompose; the last chunk has dec_wlast columns.
     uint32_t dec_wchunks = 0, dec_wlast = 0;
     std::vector<uint8_t> dec_wimg_a, dec_wimg_b;
-    std::vector<uint4> dec_fold;             // K: {p, 2^32 mod p, its Shoup companion, floor(2^32 / p)}
+    std::vector<uint4> dec_fold;             // K: {p, 2^16 mod p, its Shoup companion, floor(2^32 / p)}
 
     // Tensor-core CRT (crt_tc.cu), L >= 2: B operand, row u (a byte position of
     // X_low = sum_j y_j M_j[0 .. L-2]) and column 4j + s hold byte (u - s) of
