@@ -519,6 +519,34 @@ def main():
     c_h = np.empty((N, L), np.uint32)
     e2e_pageable_us = e2e(a_h, b_h, c_h, args.e2e_steps)
 
+    # The link itself: pinned copies of one product's operands in and result
+    # out, timed alone with CUDA events (best of 5).  Their sum plus the device
+    # time is what a synchronous call cannot beat.
+    def copy_us(dst, src, reps=5):
+        best = None
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                e0.record(stream)
+                dst.copy_(src, non_blocking=True)
+                e1.record(stream)
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) * 1e3
+            best = t if best is None else min(best, t)
+        return best
+
+    dev_in = torch.empty((2, N, L), dtype=torch.int32, device="cuda")
+    host_in = torch.empty((2, N, L), dtype=torch.int32, pin_memory=True)
+    dev_out = torch.empty((N, L), dtype=torch.int32, device="cuda")
+    h2d_us = copy_us(dev_in, host_in)
+    d2h_us = copy_us(c_pt, dev_out)
+    del dev_in, host_in, dev_out
+    link = {"h2d_gbs": 2 * N * L * 4 / (h2d_us * 1e3), "d2h_gbs": N * L * 4 / (d2h_us * 1e3),
+            "h2d_us": h2d_us, "d2h_us": d2h_us,
+            "floor_us": h2d_us + d2h_us + ms * 1e3 / args.steps,
+            "note": "pinned copies of one product's operands and result timed alone (CUDA events, best of 5); "
+                    "floor = both copies + the device time, the least a call that returns its result can take"}
+
     hbm, peak_kind = peaks()
     ab = algorithmic_bytes(N, L, K)
     kernel_bytes = {"k_decompose_pipe": ab["decompose"], "k_ntt_col_fwd": ab["ntt_col_fwd"],
@@ -582,6 +610,7 @@ def main():
                     "d2h_bytes_per_step": N * L * 4, "host_buffers": "pinned (fpm_run, wall clock)"},
             "e2e_pageable": {"value": e2e_pageable_us, "unit": "us/product",
                              "host_buffers": "pageable numpy (fpm_run stages through pinned memory)"},
+            "pcie": link,
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes": kernel_bytes[dom],
