@@ -109,11 +109,13 @@ size_t device_footprint(const HostPlan& pl) {
 
 HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2) {
     if (N < 2 || (N & (N - 1)) || N > (1u << kMaxLogN)) {
-        throw std::runtime_error("N must be a power of two in [2, 2^" + std::to_string(kMaxLogN) + "]; got " +
-                                 std::to_string(N));
+        throw std::runtime_error("unsupported transform length N = " + std::to_string(N) +
+                                 ": expected a power of two from 2 to 2^" + std::to_string(kMaxLogN));
     }
     if (L < 1 || L > kMaxL) {
-        throw std::runtime_error("L must be in [1, " + std::to_string(kMaxL) + "]; got " + std::to_string(L));
+        throw std::runtime_error("unsupported limb count L = " + std::to_string(L) + ": expected 1 to " +
+                                 std::to_string(kMaxL) + " limbs (moduli of up to " + std::to_string(32 * kMaxL) +
+                                 " bits)");
     }
     if (pmax_log2 < 24 || pmax_log2 > 31) throw std::runtime_error("prime window must be 2^24 .. 2^31");
     HostPlan pl;
@@ -127,7 +129,10 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
     pl.g = make_geometry(logN);
     pl.q.assign(q, q + L);
     const int qbits = bit_length(q, L);
-    if (qbits <= 32 * (L - 1)) throw std::runtime_error("q has fewer limbs than L");
+    if (qbits <= 32 * (L - 1)) {
+        throw std::runtime_error("modulus q has a zero top limb: its " + std::to_string(qbits) +
+                                 " bits fit in fewer than the " + std::to_string(L) + " limbs given");
+    }
     pl.q_top = modulus_top(q, L);
 
     // Primes p = 1 (mod step), step = max(2N, 2^16), from the top of the window
