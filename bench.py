@@ -61,7 +61,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="N65536_W2048")
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=50)
+    ap.add_argument("--no-configs", action="store_true", help="skip timing the other benchmark points")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched (64-product mix) measurement")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving (Poisson stream) measurement")
@@ -92,9 +93,10 @@ def peaks():
 
 
 class ClockSampler:
-    """SM clocks and clock-event (throttle) reasons, read through NVML every
-    5 ms on a background thread while the timed region runs (the same data as
-    nvidia-smi's clocks.sm and clocks_event_reasons.* queries)."""
+    """SM clocks and clock-event (throttle) reasons, read through NVML back to
+    back (about every 0.2 ms) on a background thread while the timed region
+    runs (the same data as nvidia-smi's clocks.sm and clocks_event_reasons.*
+    queries)."""
 
     NAMES = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
              "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
@@ -123,7 +125,7 @@ class ClockSampler:
             for name, bit in bits.items():
                 if r & bit:
                     self.reasons.add(name)
-            self._stop.wait(0.005)
+            self._stop.wait(0.0002)
 
     def __enter__(self):
         import threading
@@ -136,7 +138,8 @@ class ClockSampler:
         self._stop = threading.Event()
         self._thread = threading.Thread(target=self._guarded, daemon=True)
         self._thread.start()
-        time.sleep(0.02)
+        while not self.sm and not self.error and self._thread.is_alive():
+            time.sleep(0.001)   # the first sample is in before the region starts
         return self
 
     def _guarded(self):
@@ -152,27 +155,29 @@ class ClockSampler:
 
     def summary(self):
         out = {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.smax or None,
-               "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "NVML, 5 ms"}
+               "reasons": sorted(self.reasons), "samples": len(self.sm), "source": "NVML, back to back"}
         if self.error:
             out["error"] = self.error
         return out
 
 
 def algorithmic_bytes(N, L, K):
-    """Per product and per stage launch, from the six-pass RNS schedule:
-    decompose reads N L and writes K N words per operand; the column pass reads
-    and writes both operands' residues (4 K N; its K x R twiddles stay in
-    cache); the fused row pass reads 2 K N and writes K N, and reads every
-    row's prebuilt twiddle table, K x N Shoup pairs (2 K N words); the inverse
-    column pass reads and writes K N each; the CRT reads K N and writes N L."""
+    """Per product and per stage launch, from the six-pass RNS schedule with
+    twiddles cache-resident (B_alg = 4 (3 N L + 12 K N)): decompose reads N L
+    and writes K N words per operand; the column pass reads and writes both
+    operands' residues (4 K N); the fused row pass reads 2 K N and writes K N;
+    the inverse column pass reads and writes K N each; the CRT reads K N and
+    writes N L.  The row pass's prebuilt twiddle tables (K N Shoup pairs) are
+    this design's own extra traffic, reported beside the algorithmic bytes."""
     w = 4
     return {
         "decompose": w * (N * L + K * N),
         "ntt_col_fwd": w * 4 * K * N,
-        "ntt_row": w * 5 * K * N,
+        "ntt_row": w * 3 * K * N,
         "ntt_col_inv": w * 2 * K * N,
         "crt": w * (K * N + N * L),
-        "product": w * (3 * N * L + 14 * K * N),
+        "product": w * (3 * N * L + 12 * K * N),
+        "row_tables": 8 * K * N,
     }
 
 
@@ -230,6 +235,95 @@ def n65536_points(count, seed):
     seeded: the large single products as a batch."""
     rng = np.random.Generator(np.random.PCG64(seed))
     return [(65536, (1747, 2048)[i % 2], None) for i in range(count)], rng
+
+
+# The benchmark points (BASELINE configs 1-3) and their value distributions.
+CONFIG_POINTS = [
+    ("N4096_W256", "uniform"),
+    ("N32768_W868", "uniform"), ("N32768_W868", "max"), ("N32768_W868", "sparse"),
+    ("N65536_W1747", "uniform"), ("N65536_W1747", "max"),
+    ("N65536_W2048", "uniform"), ("N65536_W2048", "max"),
+]
+
+
+def measure_point(torch, polymul, workload, name, dist, stream, hbm, steps=30, e2e_steps=20):
+    """One benchmark point: device time per product (CUDA events around each
+    product, L2 flushed by a 256 MB write before each, outside the events), its
+    fraction of the HBM roofline on the algorithmic bytes, and the end-to-end
+    time through fpm_run with pinned host buffers (wall clock)."""
+    N, W = WORKLOADS[name]
+    seed = {"N4096_W256": 1, "N32768_W868": 2, "N65536_W1747": 3, "N65536_W2048": 4}[name]
+    q, a, b = workload.case(N, W, dist, seed=1000 * seed + ["uniform", "max", "sparse"].index(dist))
+    ctx = polymul.Context(N, W, q)
+    L, K = ctx.L, ctx.K
+    sp = stream.cuda_stream
+
+    def todev(x):
+        return torch.from_numpy(np.ascontiguousarray(x).view(np.int32)).to("cuda")
+
+    da, db = todev(a), todev(b)
+    dc = torch.empty_like(da)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            ctx.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sp)
+        for e0, e1 in evs:
+            flush.zero_()
+            e0.record(stream)
+            ctx.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sp)
+            e1.record(stream)
+    stream.synchronize()
+    err = ctx.get_error(sp)
+    t = sorted(e0.elapsed_time(e1) * 1e3 for e0, e1 in evs)
+    dev_us = statistics.median(t)
+
+    def pinned(x):
+        tt = torch.empty(x.shape, dtype=torch.int32, pin_memory=True)
+        v = tt.numpy().view(np.uint32)
+        v[...] = x
+        return tt, v
+
+    (ta, pa), (tb, pb), (tc, pc) = pinned(a), pinned(b), pinned(np.zeros_like(a))
+    ctx.run(pa, pb, pc)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ctx.run(pa, pb, pc)
+    e2e_us = (time.perf_counter() - t0) * 1e6 / e2e_steps
+    got = dc.cpu().numpy().view(np.uint32)
+    ab = algorithmic_bytes(N, L, K)
+    res = {"workload": name, "dist": dist, "N": N, "W": W, "L": L, "K": K,
+           "device_us": dev_us, "device_us_min": t[0], "e2e_us": e2e_us,
+           "product_algorithmic_bytes": ab["product"],
+           "hbm_frac": ab["product"] / (dev_us * 1e-6) / 1e9 / hbm,
+           "device_equals_host_path": bool(np.array_equal(got, pc)), "error_word_clear": err == 0,
+           "timing": f"median of {steps} products, L2 flushed before each; e2e {e2e_steps} fpm_run calls, "
+                     "pinned buffers, wall clock"}
+    del ta, tb, tc
+    ctx.close()
+    return res
+
+
+def measure_sustained(torch, ctx, sets_d, stream, seconds=1.0):
+    """Products back to back for about `seconds`, with the clocks sampled
+    throughout: the same step as the timed region, long enough for the clock
+    record to show the clocks under sustained load."""
+    sp = stream.cuda_stream
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n = 0
+    dev = torch.cuda.current_device()
+    with ClockSampler(dev) as clk:
+        t_end = time.perf_counter() + seconds
+        e0.record(stream)
+        while time.perf_counter() < t_end:
+            for _ in range(200):
+                da, db, dc = sets_d[n % ROTATE]
+                ctx.run_device(da.data_ptr(), db.data_ptr(), dc.data_ptr(), sp)
+                n += 1
+            stream.synchronize()
+        e1.record(stream)
+        e1.synchronize()
+    return {"products": n, "us_per_product": e0.elapsed_time(e1) * 1e3 / n, "clocks": clk.summary()}
 
 
 def measure_batched(torch, polymul, workload, stream, count=64, reps=20, mix="uneven"):
@@ -564,21 +658,30 @@ def main():
         if entry:
             traffic = entry["dram_bytes_per_launch"]
 
+    sustained = measure_sustained(torch, ctx, sets_d, stream) if rank == 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             import oracle
             if oracle.ref_available():
-                reps = 3
-                _, secs = oracle.ref_polymul(N, W, q, a_h, b_h, reps=reps)
+                reps, reps1 = 5, 3
                 cores = os.cpu_count() or 1
+                _, secs = oracle.ref_polymul(N, W, q, a_h, b_h, reps=reps, threads=cores)
+                _, secs1 = oracle.ref_polymul(N, W, q, a_h, b_h, reps=reps1, threads=1)
                 cpu = {"value": 1e6 * statistics.median(secs), "unit": "us/product", "cores": cores,
                        "kind": "reference",
-                       "sample": f"{reps} products at N={N} W={W} (median), the reference's solve_cpu.cpp "
-                                 f"(OpenMP, {cores} threads)"}
+                       "one_thread_us": 1e6 * statistics.median(secs1),
+                       "sample": f"median of {reps} products at N={N} W={W} with {cores} OpenMP threads, and of "
+                                 f"{reps1} with 1 thread (one_thread_us): the reference's solve_cpu.cpp, "
+                                 "steady_clock around fherma_run"}
         except Exception as e:  # the baseline is reported, not required
             cpu = {"value": None, "unit": "us/product", "cores": None, "kind": "reference",
                    "sample": f"failed: {e}"}
+
+    points = None
+    if rank == 0 and world == 1 and not args.no_configs:
+        points = [measure_point(torch, polymul, workload, name, dist, stream, hbm) for name, dist in CONFIG_POINTS]
 
     batched = batched_big = serving = None
     if rank == 0 and world == 1:
@@ -614,14 +717,19 @@ def main():
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes": kernel_bytes[dom],
-                         "note": "algorithmic bytes per launch / CUDA-event launch time; traffic = ncu dram "
-                                 "read+write per launch from profiles/ncu_traffic.json"},
+                         "note": "algorithmic bytes per launch (six-pass schedule, twiddles cache-resident) / "
+                                 "CUDA-event launch time, against the measured copy bandwidth; traffic = ncu "
+                                 "dram read+write per launch from profiles/ncu_traffic.json (includes the row "
+                                 "pass's own twiddle-table reads)"},
             "stages_us": stages,
             "kernels_us": kernels,
             "product_algorithmic_bytes": ab["product"],
+            "row_table_bytes": ab["row_tables"],
             "product_hbm_frac": ab["product"] / (us_per_product * world * 1e-6) / 1e9 / hbm,
             "gpu_launches": args.steps * launches_per_product,
             "clocks": clocks,
+            "sustained": sustained,
+            "configs": points,
             "cpu_baseline": cpu,
             "batched": batched,
             "batched_n65536": batched_big,

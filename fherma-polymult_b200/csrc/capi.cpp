@@ -50,6 +50,8 @@ int guarded(F&& f) {
         return FPM_OK;
     } catch (const std::bad_alloc&) {
         return fail(FPM_ENOMEM, "out of host memory");
+    } catch (const fpm::PipelineTimeout& e) {
+        return fail(FPM_ETIMEOUT, e.what());
     } catch (const fpm::CudaError& e) {
         return fail(e.code == cudaErrorMemoryAllocation ? FPM_ENOMEM : FPM_ECUDA, e.what());
     } catch (const std::runtime_error& e) {
@@ -94,8 +96,10 @@ int fpm_init_ex(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int prime
     if (!out) return fail(FPM_EINVAL, "fpm_init: out is NULL");
     *out = nullptr;
     if (!q) return fail(FPM_EINVAL, "fpm_init: q is NULL");
-    if (L < 1 || L > static_cast<uint32_t>(fpm::kMaxL))
-        return fail(FPM_EINVAL, "L must be in [1, " + std::to_string(fpm::kMaxL) + "]; got " + std::to_string(L));
+    if (L < 1 || L > static_cast<uint32_t>(fpm::kMaxL)) {
+        return fail(FPM_EINVAL, "unsupported limb count L = " + std::to_string(L) + ": expected 1 to " +
+                                    std::to_string(fpm::kMaxL));
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -123,6 +127,44 @@ int fpm_run_device(fpm_ctx* ctx, const uint32_t* d_a, const uint32_t* d_b, uint3
 int fpm_run_device_noalloc(fpm_ctx* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, void* stream) {
     if (!ctx || !d_a || !d_b || !d_c) return fail(FPM_EINVAL, "fpm_run_device_noalloc: NULL argument");
     return guarded([&] { ctx->engine->run_device_static(d_a, d_b, d_c, as_stream(stream)); });
+}
+
+namespace {
+
+int timeout_status(uint32_t word, const char* where) {
+    if (!word) return FPM_OK;
+    return fail(FPM_ETIMEOUT, std::string(where) + ": a kernel pipeline wait ran out of time (error word " +
+                                  std::to_string(word) + "); the products enqueued since the last check are not "
+                                  "valid");
+}
+
+}  // namespace
+
+int fpm_get_error(fpm_ctx* ctx, void* stream) {
+    if (!ctx) return fail(FPM_EINVAL, "fpm_get_error: NULL context");
+    uint32_t word = 0;
+    const int rc = guarded([&] { word = ctx->engine->take_error(as_stream(stream)); });
+    return rc ? rc : timeout_status(word, "fpm_get_error");
+}
+
+int fpm_noalloc_get_error(void* stream) {
+    uint32_t word = 0;
+    const int rc = guarded([&] { word = fpm::Engine::take_static_error(as_stream(stream)); });
+    return rc ? rc : timeout_status(word, "fpm_noalloc_get_error");
+}
+
+int fpm_set_wait_limit(fpm_ctx* ctx, uint64_t ns) {
+    if (!ctx) return fail(FPM_EINVAL, "fpm_set_wait_limit: NULL context");
+    if (ns == 0) return fail(FPM_EINVAL, "fpm_set_wait_limit: the limit must be positive");
+    ctx->engine->set_wait_limit(ns);
+    return FPM_OK;
+}
+
+int fpm_debug_inject_stall(fpm_ctx* ctx, uint32_t mask) {
+    if (!ctx) return fail(FPM_EINVAL, "fpm_debug_inject_stall: NULL context");
+    if (mask & ~3u) return fail(FPM_EINVAL, "fpm_debug_inject_stall: mask bits are 1 (decompose) and 2 (CRT)");
+    ctx->engine->set_fault(mask);
+    return FPM_OK;
 }
 
 void fpm_free(fpm_ctx* ctx) {

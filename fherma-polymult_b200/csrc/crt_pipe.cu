@@ -13,65 +13,59 @@
 // 2^20 N q^2, so sum_j y_j / p_j lies within 2^-21 of an integer and a
 // fixed-point sum with r_j = floor(2^50 / p_j) (error below 2^-11) rounds to v.
 //
-// Organisation on the B200:
-//   * one CTA per SM walks super-tiles of 256 coefficients; TMEM's 512 columns
-//     hold the two 128-row halves of a super-tile (U <= 256 columns each);
-//   * warp 0 (one thread) streams the constant image in, chunk by chunk,
-//     through a two-slot ring;
-//   * warps 2-9, one thread per row, load y straight from HBM (coalesced,
-//     the next chunk's loads in flight under the current chunk's work), write
-//     it into the MMA's K-major byte layout, add up the rounding sum and the
-//     top limb, and put v in the last chunk;
-//   * warp 1 (one thread) issues the MMAs, two halves per chunk;
-//   * warps 10-17, one thread per row: a quotient estimate e from the top
-//     TMEM columns (within one of floor(X / q)), then one pass from the bottom
-//     limb up that assembles X from D with carries, subtracts e q, stores the
-//     limbs and tracks the borrows that tell whether X - e q lies in [0, q);
-//     the rare row that does not (about 2^-11 of them) adds or subtracts q in
-//     a second pass over what it stored.
-// Per-prime constants and q come from kernel parameters (constant bank), so
-// shared memory carries only the MMA operands and the per-row top limbs.
+// Organisation on the B200: one CTA per SM walks tiles of 128 coefficients
+// (one MMA M); tile i of a CTA accumulates into TMEM buffer i % 2 (256 columns
+// each), so a tile's epilogue overlaps the next tile's staging and MMAs:
+//   * warp 0 (one thread) streams the constant image, chunk by chunk (32
+//     primes, U x 128 bytes), through a two-slot ring (bulk copies, L2-resident);
+//   * warp 2 (one thread) streams y through a three-slot ring with 2-D TMA
+//     copies: per chunk a box of 32 primes x 128 coefficients (16 KB) of the
+//     prime-major K x N array;
+//   * warps 3-6, one thread per row, read their row's 32 values of a chunk from
+//     the ring (conflict-free), write them in the MMA's K-major byte layout
+//     (two-slot A ring), add up the rounding sum and the top limb, and put v in
+//     the last chunk;
+//   * warp 1 (one thread) issues a chunk's MMAs as soon as its A and B slots
+//     are full;
+//   * warps 7-10 and 11-14 are two epilogue groups, one per TMEM buffer, one
+//     thread per row: a quotient estimate e from the top TMEM columns (within
+//     one of floor(X / q)), then one pass from the bottom limb up that
+//     assembles X from D with carries, subtracts e q, and tracks the borrows
+//     that tell whether X - e q lies in [0, q); the rare row that does not
+//     (about 2^-11 of them) adds or subtracts q in a second pass over its
+//     staged limbs.  Rows are staged in padded shared memory and a group copies
+//     its tile's 128 rows (one contiguous run of c) out with coalesced stores.
+// Per-prime constants and q come from kernel parameters (constant bank).
 // The kernel is compiled for the common limb counts (L = 64, 55, 28, 8) and
 // once for any L.
 //
-// Every wait is bounded; a timeout raises an abort flag that every role
-// checks, the producer and the MMA thread wait out what they have in flight,
-// and the error word gets bit 1.
+// Every wait is bounded (DevPoint::wait_ns); a timeout raises an abort flag
+// that every role checks, the copy and MMA issuers wait out what they have in
+// flight, and the error word gets bit 1.
 #include "device.cuh"
 #include "kernels.h"
 #include "pdl.cuh"
 #include "tc.cuh"
+#include "tmap.h"
 
 namespace fpm {
 
 namespace {
 
-constexpr int kThreads = 576;             // 18 warps
-constexpr int kStagerWarp0 = 2;           // warps 2-9
-constexpr int kEpiWarp0 = 10;             // warps 10-17
-constexpr uint32_t kSuper = 256;          // coefficients per super-tile
+constexpr int kThreads = 480;             // 15 warps
+constexpr int kBWarp = 0;
+constexpr int kMmaWarp = 1;
+constexpr int kYWarp = 2;
+constexpr int kStagerWarp0 = 3;           // warps 3-6
+constexpr int kEpiWarp0 = 7;              // warps 7-10 (group 0), 11-14 (group 1)
+constexpr uint32_t kCrtTile = 128;           // coefficients per tile
 constexpr uint32_t kChunk = 32;           // K rows (primes) per chunk
 constexpr int kMaxChunks = kMaxK / kChunk;   // K + 1 <= kMaxK rows
-constexpr uint32_t kSlot = 32768;         // bytes: A slot (two halves), B slot (U <= 256)
+constexpr int kYStages = 3;
+constexpr uint32_t kBSlot = 32768;        // U <= 256 rows of 128 bytes
+constexpr uint32_t kASlot = 16384;        // [8 core columns][128 rows][16 bytes]
+constexpr uint32_t kYSlot = kChunk * kCrtTile * 4;   // [32 primes][128 coefficients] u32
 constexpr int kX = kMaxL + 2;
-
-struct Smem {
-    uint8_t* a;          // [2][2 halves][16 KB]
-    uint8_t* b;          // [2][U x 128]
-    uint4* meta;         // [2][256] {top limb words 0, 1, 2, -}
-    uint32_t* outs;      // [2 halves][128 rows][out_stride(L)] result limbs
-    uint64_t* b_full;    // [2]
-    uint64_t* a_full;    // [2]
-    uint64_t* mma_done;  // [2]
-    uint64_t* d_full;    // [1]
-    uint64_t* d_empty;   // [2]
-    uint64_t* m_full;    // [2]
-    uint64_t* m_empty;   // [2]
-    uint64_t* o_ready;   // [2] a half's result rows are in outs
-    uint64_t* o_free;    // [2] a half's rows have been copied out
-    uint32_t* tmem_base;
-    volatile uint32_t* abort;
-};
 
 // Words per staged result row: a 16-byte-chunk stride that is odd (vector
 // rows, L a multiple of 4) or an odd word stride (scalar rows), so the
@@ -79,51 +73,59 @@ struct Smem {
 __host__ __device__ constexpr int out_stride(int L) { return (L & 3) == 0 ? 4 * ((L / 4) | 1) : (L | 1); }
 constexpr int kMaxOutStride = out_stride(kMaxL);
 
-constexpr size_t kMetaOff = 4 * size_t(kSlot);
-constexpr size_t kOutOff = kMetaOff + 2 * kSuper * sizeof(uint4);
-constexpr size_t kBarOff = kOutOff + size_t(kSuper) * kMaxOutStride * 4;
-constexpr size_t kSmemBytes = kBarOff + 17 * 8 + 16;
+constexpr size_t kBOff = 0;
+constexpr size_t kAOff = kBOff + 2 * size_t(kBSlot);
+constexpr size_t kYOff = kAOff + 2 * size_t(kASlot);
+constexpr size_t kMetaOff = kYOff + kYStages * size_t(kYSlot);
+constexpr size_t kOutOff = kMetaOff + 2 * kCrtTile * sizeof(uint4);
+constexpr size_t kBarOff = kOutOff + 2 * size_t(kCrtTile) * kMaxOutStride * 4;
+constexpr int kBars = 2 + 2 + 2 + 2 + 2 * kYStages + 2 + 2 + 2 + 2 + 2;
+constexpr size_t kSmemBytes = kBarOff + kBars * 8 + 16;
+static_assert(kSmemBytes <= 227 * 1024, "shared memory budget");
+
+struct Smem {
+    uint8_t* b;          // [2][kBSlot]
+    uint8_t* a;          // [2][kASlot]
+    uint32_t* y;         // [kYStages][32][128]
+    uint4* meta;         // [2][128] {top-limb words 0, 1, 2, -}
+    uint32_t* outs;      // [2 groups][128 rows][out_stride(L)] result limbs
+    uint64_t* b_full;    // [2] constant chunk landed
+    uint64_t* b_empty;   // [2] its MMAs finished
+    uint64_t* a_full;    // [2] 128 rows staged
+    uint64_t* a_empty;   // [2] its MMAs finished
+    uint64_t* y_full;    // [kYStages] TMA box landed
+    uint64_t* y_empty;   // [kYStages] 128 rows read it
+    uint64_t* d_full;    // [2] a tile's MMAs finished (per TMEM buffer)
+    uint64_t* d_empty;   // [2] its epilogue group has read TMEM
+    uint64_t* m_full;    // [2] a tile's top-limb words staged
+    uint64_t* m_empty;   // [2] and read
+    uint64_t* o_sync;    // [2] per-group barrier (128 arrivals)
+    uint32_t* tmem_base;
+    volatile uint32_t* abort;
+};
 
 __device__ inline Smem carve(uint8_t* base) {
     Smem s;
-    s.a = base;
-    s.b = base + 2 * kSlot;
+    s.b = base + kBOff;
+    s.a = base + kAOff;
+    s.y = reinterpret_cast<uint32_t*>(base + kYOff);
     s.meta = reinterpret_cast<uint4*>(base + kMetaOff);
     s.outs = reinterpret_cast<uint32_t*>(base + kOutOff);
     uint64_t* bars = reinterpret_cast<uint64_t*>(base + kBarOff);
     s.b_full = bars;
-    s.a_full = bars + 2;
-    s.mma_done = bars + 4;
-    s.d_full = bars + 6;
-    s.d_empty = bars + 7;
-    s.m_full = bars + 9;
-    s.m_empty = bars + 11;
-    s.o_ready = bars + 13;
-    s.o_free = bars + 15;
-    s.tmem_base = reinterpret_cast<uint32_t*>(bars + 17);
+    s.b_empty = bars + 2;
+    s.a_full = bars + 4;
+    s.a_empty = bars + 6;
+    s.y_full = bars + 8;
+    s.y_empty = bars + 8 + kYStages;
+    s.d_full = bars + 8 + 2 * kYStages;
+    s.d_empty = s.d_full + 2;
+    s.m_full = s.d_full + 4;
+    s.m_empty = s.d_full + 6;
+    s.o_sync = s.d_full + 8;
+    s.tmem_base = reinterpret_cast<uint32_t*>(bars + kBars);
     s.abort = s.tmem_base + 1;
     return s;
-}
-
-// y_j of one coefficient, streamed past L1.
-__device__ __forceinline__ uint32_t ld_stream(const uint32_t* p) {
-    uint32_t v;
-    asm volatile("ld.global.nc.L1::no_allocate.b32 %0, [%1];" : "=r"(v) : "l"(p));
-    return v;
-}
-
-// Bounded wait that also gives up once another role has raised the abort flag.
-__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile uint32_t* abort) {
-    if (tc::mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = tc::globaltimer();
-    while (!tc::mbar_try_wait_sleep(bar, parity)) {
-        if (*abort) return false;
-        if (tc::globaltimer() - t0 > tc::kWaitNs) {
-            *abort = 1;
-            return false;
-        }
-    }
-    return true;
 }
 
 // Waits for this thread's TMEM loads; naming the registers keeps every read of
@@ -140,7 +142,7 @@ __device__ __forceinline__ void tmem_wait(uint32_t (&r)[16]) {
 // LT > 0: L = LT at compile time; LT = 0: any L (predicated).
 template <int LT>
 __global__ void __launch_bounds__(kThreads, 1)
-    k_crt_pipe(DevPoint d, const __grid_constant__ CrtConsts cc, const uint32_t* __restrict__ Y,
+    k_crt_pipe(DevPoint d, const __grid_constant__ CrtConsts cc, const __grid_constant__ CUtensorMap tmY,
                uint32_t* __restrict__ C, uint32_t n_begin, uint32_t n_end) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     pdl_launch_dependents();
@@ -149,131 +151,148 @@ __global__ void __launch_bounds__(kThreads, 1)
     const int L = LT > 0 ? LT : d.L;
     const int K = d.K;
     const uint32_t U = LT > 0 ? (4 * LT - 1 + 31) / 32 * 32 : d.crt_u;
-    const uint32_t N = d.N;
     const int nch = (K + 1 + static_cast<int>(kChunk) - 1) / static_cast<int>(kChunk);   // K + 1 rows
-    const uint32_t tiles = (n_end - n_begin + kSuper - 1) / kSuper;
+    const uint32_t tiles = (n_end - n_begin + kCrtTile - 1) / kCrtTile;
+    const uint64_t lim = d.wait_ns;
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < 2; ++i) {
             tc::mbar_init(&sm.b_full[i], 1);
-            tc::mbar_init(&sm.a_full[i], 256);
-            tc::mbar_init(&sm.mma_done[i], 1);
-            tc::mbar_init(&sm.d_empty[i], 128);
-            tc::mbar_init(&sm.m_full[i], 256);
-            tc::mbar_init(&sm.m_empty[i], 256);
-            tc::mbar_init(&sm.o_ready[i], 128);
-            tc::mbar_init(&sm.o_free[i], 128);
+            tc::mbar_init(&sm.b_empty[i], 1);
+            tc::mbar_init(&sm.a_full[i], kCrtTile);
+            tc::mbar_init(&sm.a_empty[i], 1);
+            tc::mbar_init(&sm.d_full[i], 1);
+            tc::mbar_init(&sm.d_empty[i], kCrtTile);
+            tc::mbar_init(&sm.m_full[i], kCrtTile);
+            tc::mbar_init(&sm.m_empty[i], kCrtTile);
+            tc::mbar_init(&sm.o_sync[i], kCrtTile);
         }
-        tc::mbar_init(sm.d_full, 1);
+        for (int i = 0; i < kYStages; ++i) {
+            tc::mbar_init(&sm.y_full[i], 1);
+            tc::mbar_init(&sm.y_empty[i], kCrtTile);
+        }
         *sm.abort = 0;
         tc::fence_mbar_init();
     }
+    if (warp == kYWarp && lane == 0) tc::prefetch_tmap(&tmY);
     if (warp == 0) tc::tmem_alloc(sm.tmem_base, 512);
     tc::tc_fence_before();
     __syncthreads();
     tc::tc_fence_after();
     const uint32_t tmem = *sm.tmem_base;
-    pdl_wait();   // y and c belong to the kernels around this one
 
-    if (warp == 0) {
-        // ---- producer: constant chunks, two-slot ring ----
+    if (warp == kBWarp) {
+        // ---- constant chunks (read-only plan data: no wait for the
+        // preceding kernel) ----
         if (lane == 0) {
             const uint32_t bbytes = U * 128;
-            uint32_t b_par[2] = {0, 0};   // parity of each slot's last arming
-            bool armed_b[2] = {false, false};
+            uint32_t par[2] = {0, 0};
+            bool armed[2] = {false, false};
             uint32_t g = 0;
-            for (uint32_t t = blockIdx.x; t < tiles && !*sm.abort; t += gridDim.x) {
+            bool ok = true;
+            for (uint32_t t = blockIdx.x; ok && t < tiles; t += gridDim.x) {
                 for (int c = 0; c < nch; ++c, ++g) {
                     const int s = g & 1;
-                    if (g >= 2 && !wait_or_abort(&sm.mma_done[s], ((g - 2) >> 1) & 1, sm.abort)) break;
+                    if (g >= 2 && !(ok = tc::wait_or_abort(&sm.b_empty[s], ((g - 2) >> 1) & 1, sm.abort, lim))) break;
+                    if (g == 0 && (d.fault & kFaultCrt)) continue;   // test hook: this phase never completes
                     tc::mbar_arrive_expect_tx(&sm.b_full[s], bbytes);
-                    tc::bulk_g2s(sm.b + s * kSlot, d.crt_img_v + static_cast<size_t>(c) * bbytes, bbytes,
+                    tc::bulk_g2s(sm.b + s * kBSlot, d.crt_img_v + static_cast<size_t>(c) * bbytes, bbytes,
                                  &sm.b_full[s]);
-                    b_par[s] = (g >> 1) & 1;
-                    armed_b[s] = true;
+                    par[s] = (g >> 1) & 1;
+                    armed[s] = true;
                 }
-                if (*sm.abort) break;
             }
             // Copies still in flight must land before the CTA may exit.
             for (int s = 0; s < 2; ++s) {
-                if (armed_b[s]) tc::wait_parity(&sm.b_full[s], b_par[s]);
+                if (armed[s]) tc::wait_parity(&sm.b_full[s], par[s], lim);
             }
         }
         __syncwarp();
-    } else if (warp == 1) {
+    } else if (warp == kYWarp) {
+        // ---- y boxes through the TMA ring ----
+        if (lane == 0) {
+            pdl_wait();   // y is the preceding kernel's output
+            uint32_t par[kYStages] = {};
+            bool armed[kYStages] = {};
+            uint32_t g = 0;
+            bool ok = true;
+            for (uint32_t t = blockIdx.x; ok && t < tiles; t += gridDim.x) {
+                const int x = static_cast<int>(n_begin + t * kCrtTile);
+                for (int c = 0; c < nch; ++c, ++g) {
+                    const uint32_t s = g % kYStages, u = g / kYStages;
+                    if (u >= 1 && !(ok = tc::wait_or_abort(&sm.y_empty[s], (u - 1) & 1, sm.abort, lim))) break;
+                    tc::mbar_arrive_expect_tx(&sm.y_full[s], kYSlot);
+                    tc::tma_load_2d(sm.y + s * (kYSlot / 4), &tmY, x, c * static_cast<int>(kChunk), &sm.y_full[s]);
+                    par[s] = u & 1;
+                    armed[s] = true;
+                }
+            }
+            for (int s = 0; s < kYStages; ++s) {
+                if (armed[s]) tc::wait_parity(&sm.y_full[s], par[s], lim);
+            }
+        }
+        __syncwarp();
+    } else if (warp == kMmaWarp) {
         // ---- MMA issuer ----
         if (lane == 0) {
             const uint32_t idesc = tc::idesc_u8(U);
-            uint32_t g = 0, it = 0;
-            bool issued = false;
-            uint32_t last_s = 0, last_par = 0;
-            for (uint32_t t = blockIdx.x; t < tiles && !*sm.abort; t += gridDim.x, ++it) {
-                bool ok = true;
-                if (it >= 1) {
-                    ok = wait_or_abort(&sm.d_empty[0], (it - 1) & 1, sm.abort) &&
-                         wait_or_abort(&sm.d_empty[1], (it - 1) & 1, sm.abort);
-                }
-                for (int c = 0; c < nch && ok; ++c, ++g) {
+            uint32_t g = 0, i = 0;
+            uint64_t* last_bar = nullptr;
+            uint32_t last_par = 0;
+            bool ok = true;
+            for (uint32_t t = blockIdx.x; ok && t < tiles; t += gridDim.x, ++i) {
+                const uint32_t buf = i & 1, use = i >> 1;
+                if (use >= 1 && !(ok = tc::wait_or_abort(&sm.d_empty[buf], (use - 1) & 1, sm.abort, lim))) break;
+                for (int c = 0; c < nch; ++c, ++g) {
                     const int s = g & 1;
-                    ok = wait_or_abort(&sm.b_full[s], (g >> 1) & 1, sm.abort) &&
-                         wait_or_abort(&sm.a_full[s], (g >> 1) & 1, sm.abort);
+                    const uint32_t ph = (g >> 1) & 1;
+                    ok = tc::wait_or_abort(&sm.b_full[s], ph, sm.abort, lim) &&
+                         tc::wait_or_abort(&sm.a_full[s], ph, sm.abort, lim);
                     if (!ok) break;
                     tc::tc_fence_after();
-                    const uint32_t a0 = tc::smem_addr(sm.a + s * kSlot), b0 = tc::smem_addr(sm.b + s * kSlot);
+                    const uint32_t a0 = tc::smem_addr(sm.a + s * kASlot), b0 = tc::smem_addr(sm.b + s * kBSlot);
                     // K steps of 8 rows; the last chunk stops after row K.
                     const int rows_c = min(static_cast<int>(kChunk), K + 1 - c * static_cast<int>(kChunk));
                     const uint32_t ksteps = static_cast<uint32_t>(rows_c + 7) / 8;
-                    for (uint32_t h = 0; h < 2; ++h) {
-                        for (uint32_t kk = 0; kk < ksteps; ++kk) {
-                            const uint64_t ad = tc::smem_desc(a0 + h * 16384 + kk * 2 * 2048, 2048, 128);
-                            const uint64_t bd = tc::smem_desc(b0 + kk * 2 * (U * 16), U * 16, 128);
-                            tc::mma_u8(tmem + h * 256, ad, bd, idesc, c > 0 || kk > 0);
-                        }
+                    for (uint32_t kk = 0; kk < ksteps; ++kk) {
+                        const uint64_t ad = tc::smem_desc(a0 + kk * 2 * 2048, 2048, 128);
+                        const uint64_t bd = tc::smem_desc(b0 + kk * 2 * (U * 16), U * 16, 128);
+                        tc::mma_u8(tmem + buf * 256, ad, bd, idesc, c > 0 || kk > 0);
                     }
-                    tc::mma_commit(&sm.mma_done[s]);
-                    issued = true;
-                    last_s = s;
-                    last_par = (g >> 1) & 1;
+                    tc::mma_commit(&sm.a_empty[s]);
+                    tc::mma_commit(&sm.b_empty[s]);
+                    last_bar = &sm.b_empty[s];
+                    last_par = ph;
                 }
                 if (!ok) break;
-                tc::mma_commit(sm.d_full);
+                tc::mma_commit(&sm.d_full[buf]);
             }
             // MMAs still running must finish before the CTA may exit.
-            if (issued) tc::wait_parity(&sm.mma_done[last_s], last_par);
+            if (last_bar) tc::wait_parity(last_bar, last_par, lim);
         }
         __syncwarp();
     } else if (warp < kEpiWarp0) {
-        // ---- stagers: thread = one row of the super-tile ----
-        const uint32_t row = threadIdx.x - kStagerWarp0 * 32;
-        const uint32_t h = row >> 7, m = row & 127;
-        uint32_t g = 0, it = 0;
-        for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
-            const uint32_t n0 = n_begin + t * kSuper;
-            const bool live = row < min(kSuper, n_end - n0);
-            const uint32_t* yrow = Y + n0 + row;
+        // ---- stagers: thread = one row of the tile ----
+        pdl_wait();
+        const uint32_t m = threadIdx.x - kStagerWarp0 * 32;
+        uint32_t g = 0, i = 0;
+        for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++i) {
+            const uint32_t n0 = n_begin + t * kCrtTile;
+            const bool live = m < min(kCrtTile, n_end - n0);
             uint64_t vacc = 0, tlo = 0, thi = 0;   // sum y r50; sum y (top & 0xFFFF); sum y (top >> 16)
             bool ok = true;
-            uint32_t ya[kChunk], yb[kChunk];
-#pragma unroll
-            for (int jj = 0; jj < static_cast<int>(kChunk); ++jj)
-                ya[jj] = (live && jj < K) ? ld_stream(yrow + static_cast<size_t>(jj) * N) : 0u;
 #pragma unroll
             for (int c = 0; c < kMaxChunks; ++c) {
                 if (c >= nch) break;
-                uint32_t(&yv)[kChunk] = (c & 1) ? yb : ya;
-                uint32_t(&yn)[kChunk] = (c & 1) ? ya : yb;
-                if (c + 1 < kMaxChunks && c + 1 < nch) {
-                    // The next chunk's loads go out before this chunk's work.
-#pragma unroll
-                    for (int jj = 0; jj < static_cast<int>(kChunk); ++jj) {
-                        const int j = (c + 1) * static_cast<int>(kChunk) + jj;
-                        yn[jj] = (live && j < K) ? ld_stream(yrow + static_cast<size_t>(j) * N) : 0u;
-                    }
-                }
-                const int s = g & 1;
-                if (g >= 2) ok = wait_or_abort(&sm.mma_done[s], ((g - 2) >> 1) & 1, sm.abort);
+                uint32_t yv[kChunk];
+                const uint32_t ys = g % kYStages, yu = g / kYStages;
+                ok = tc::wait_or_abort(&sm.y_full[ys], yu & 1, sm.abort, lim);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
+                const uint32_t* yrow = sm.y + ys * (kYSlot / 4) + m;
+#pragma unroll
+                for (int jj = 0; jj < static_cast<int>(kChunk); ++jj) yv[jj] = yrow[jj * kCrtTile];
+                tc::mbar_arrive(&sm.y_empty[ys]);
 #pragma unroll
                 for (int jj = 0; jj < static_cast<int>(kChunk); ++jj) {
                     const int j = c * static_cast<int>(kChunk) + jj;
@@ -294,7 +313,13 @@ __global__ void __launch_bounds__(kThreads, 1)
                     for (int jj = 0; jj < static_cast<int>(kChunk); ++jj)
                         if (c * static_cast<int>(kChunk) + jj == K) yv[jj] = vu;
                 }
-                uint8_t* as = sm.a + s * kSlot + h * 16384 + m * 16;
+                const int s = g & 1;
+                if (g >= 2) {
+                    ok = tc::wait_or_abort(&sm.a_empty[s], ((g - 2) >> 1) & 1, sm.abort, lim);
+                    ok = __all_sync(0xffffffffu, ok);
+                    if (!ok) break;
+                }
+                uint8_t* as = sm.a + s * kASlot + m * 16;
 #pragma unroll
                 for (int q4 = 0; q4 < 8; ++q4)
                     *reinterpret_cast<uint4*>(as + q4 * 2048) =
@@ -304,46 +329,46 @@ __global__ void __launch_bounds__(kThreads, 1)
                 ++g;
             }
             if (!ok) break;
-            const int p = it & 1;
-            if (it >= 2) {
-                ok = wait_or_abort(&sm.m_empty[p], ((it - 2) >> 1) & 1, sm.abort);
+            const int p = i & 1;
+            if (i >= 2) {
+                ok = tc::wait_or_abort(&sm.m_empty[p], ((i - 2) >> 1) & 1, sm.abort, lim);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
             }
             // Top-limb sum = tlo + thi 2^16, as three words.
             const uint64_t t0 = tlo + ((thi & 0xFFFFu) << 16);
             const uint64_t t1 = (t0 >> 32) + (thi >> 16);
-            sm.meta[p * kSuper + row] =
+            sm.meta[p * kCrtTile + m] =
                 make_uint4(static_cast<uint32_t>(t0), static_cast<uint32_t>(t1), static_cast<uint32_t>(t1 >> 32), 0u);
             tc::mbar_arrive(&sm.m_full[p]);
         }
     } else {
-        // ---- epilogue: thread = one row of one half ----
-        const int ew = warp - kEpiWarp0;
-        const uint32_t h = ew >> 2, qd = warp & 3;
-        const uint32_t row = h * 128 + qd * 32 + lane;
-        const uint32_t tq = tmem + ((qd * 32) << 16) + h * 256;
+        // ---- epilogue group grp (TMEM buffer grp): thread = one row ----
+        pdl_wait();
+        const uint32_t grp = static_cast<uint32_t>(warp - kEpiWarp0) >> 2, qd = warp & 3;
+        const uint32_t row = qd * 32 + lane;
+        const uint32_t tq = tmem + ((qd * 32) << 16) + grp * 256;
         const uint32_t npieces = U / 16;
         const int n = L + 2, drop = top_drop(L);
         const uint32_t top_piece = static_cast<uint32_t>(4 * drop) / 16;
         const bool svec = (L & 3) == 0;                                             // 16-byte rows in outs
         const bool gvec = svec && (reinterpret_cast<uintptr_t>(C) & 15) == 0;      // 16-byte global stores
         const int ostride = LT > 0 ? out_stride(LT) : out_stride(L);
-        const uint32_t hrow = qd * 32 + lane;                                       // row within the half
-        uint32_t* srow = sm.outs + (h * 128 + hrow) * ostride;
+        uint32_t* const obase = sm.outs + grp * kCrtTile * ostride;
+        uint32_t* srow = obase + row * ostride;
         constexpr int kXL = LT > 0 ? LT + 2 : kX;        // limbs handled
         constexpr int kPieces = (kXL + 3) / 4;
-        uint32_t it = 0;
-        for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
-            const uint32_t n0 = n_begin + t * kSuper;
-            const bool live = row < min(kSuper, n_end - n0);
-            const int p = it & 1;
-            bool ok = wait_or_abort(&sm.m_full[p], (it >> 1) & 1, sm.abort);
+        uint32_t k = 0;   // this group's tiles so far
+        for (uint32_t t = blockIdx.x + grp * gridDim.x; t < tiles; t += 2 * gridDim.x, ++k) {
+            const uint32_t n0 = n_begin + t * kCrtTile;
+            const uint32_t rows_t = min(kCrtTile, n_end - n0);
+            const bool live = row < rows_t;
+            bool ok = tc::wait_or_abort(&sm.m_full[grp], k & 1, sm.abort, lim);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) break;
-            const uint4 meta = sm.meta[p * kSuper + row];
-            tc::mbar_arrive(&sm.m_empty[p]);
-            ok = wait_or_abort(sm.d_full, it & 1, sm.abort);
+            const uint4 meta = sm.meta[grp * kCrtTile + row];
+            tc::mbar_arrive(&sm.m_empty[grp]);
+            ok = tc::wait_or_abort(&sm.d_full[grp], k & 1, sm.abort, lim);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) break;
             tc::tc_fence_after();
@@ -355,7 +380,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tc::tmem_ld16(tq + pc * 16, ra);
                 tmem_wait(ra);
 #pragma unroll
-                for (int k = 15; k >= 0; --k) xd = xd * 256.0 + ra[k];
+                for (int kk = 15; kk >= 0; --kk) xd = xd * 256.0 + ra[kk];
             }
             xd = ldexp(xd, static_cast<int>(8 * 16 * top_piece) - 32 * drop) +
                  ldexp(static_cast<double>(meta.x), 32 * (L - 1 - drop)) +
@@ -364,12 +389,6 @@ __global__ void __launch_bounds__(kThreads, 1)
             const double f = floor(xd * d.q_top_inv);
             const uint64_t e = f > 0 ? static_cast<uint64_t>(f) : 0;
             const uint32_t e_lo = static_cast<uint32_t>(e), e_hi = static_cast<uint32_t>(e >> 32);
-            if (it >= 1) {
-                // The previous super-tile's rows of this half have left outs.
-                ok = wait_or_abort(&sm.o_free[h], (it - 1) & 1, sm.abort);
-                ok = __all_sync(0xffffffffu, ok);
-                if (!ok) break;
-            }
             // One pass from the bottom: X with carries, minus e q; the borrows
             // of X - e q (b0) and of (X - e q) - q (b1).  TMEM pieces are
             // double-buffered: piece pc + 1 loads while piece pc is used.
@@ -386,21 +405,21 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const bool more = static_cast<uint32_t>(pc + 1) < npieces;
                 if (more) tc::tmem_ld16(tq + (pc + 1) * 16, nxt);
 #pragma unroll
-                for (int i = 0; i < 4; ++i) {
-                    const int k = 4 * pc + i;
-                    if (k < kXL && k < n) {
+                for (int ii = 0; ii < 4; ++ii) {
+                    const int kl = 4 * pc + ii;
+                    if (kl < kXL && kl < n) {
                         uint64_t w = carry;
                         if (have) {
-                            w += cur[4 * i];
-                            w += static_cast<uint64_t>(cur[4 * i + 1]) * 256u;
-                            w += static_cast<uint64_t>(cur[4 * i + 2]) * 65536u;
-                            w += static_cast<uint64_t>(cur[4 * i + 3]) * 16777216u;
+                            w += cur[4 * ii];
+                            w += static_cast<uint64_t>(cur[4 * ii + 1]) * 256u;
+                            w += static_cast<uint64_t>(cur[4 * ii + 2]) * 65536u;
+                            w += static_cast<uint64_t>(cur[4 * ii + 3]) * 16777216u;
                         }
-                        if (k == L - 1) w += meta.x;
-                        if (k == L) w += meta.y;
-                        if (k == L + 1) w += meta.z;
+                        if (kl == L - 1) w += meta.x;
+                        if (kl == L) w += meta.y;
+                        if (kl == L + 1) w += meta.z;
                         carry = w >> 32;
-                        const uint32_t qk = cc.q[k];
+                        const uint32_t qk = cc.q[kl];
                         const uint64_t acc = static_cast<uint64_t>(e_lo) * qk + c0;
                         c0 = (acc >> 32) + static_cast<uint64_t>(e_hi) * qk;
                         const uint64_t dy =
@@ -408,63 +427,65 @@ __global__ void __launch_bounds__(kThreads, 1)
                         const uint32_t yk = static_cast<uint32_t>(dy);
                         b0 = static_cast<uint32_t>(dy >> 63);
                         b1 = static_cast<uint32_t>((static_cast<uint64_t>(yk) - qk - b1) >> 63);
-                        o[i] = yk;
-                        if (k < L) {
+                        o[ii] = yk;
+                        if (kl < L) {
                             if (svec) {
-                                if (i == 3) *reinterpret_cast<uint4*>(srow + k - 3) = make_uint4(o[0], o[1], o[2], o[3]);
+                                if (ii == 3) *reinterpret_cast<uint4*>(srow + kl - 3) = make_uint4(o[0], o[1], o[2], o[3]);
                             } else {
-                                srow[k] = yk;
+                                srow[kl] = yk;
                             }
                         }
                     }
                 }
                 if (more) tmem_wait(nxt);
             }
-            // TMEM is read: the next super-tile's MMAs may start on this half.
+            // TMEM is read: the MMAs of this buffer's next tile may start.
             tc::tc_fence_before();
-            tc::mbar_arrive(&sm.d_empty[h]);
+            tc::mbar_arrive(&sm.d_empty[grp]);
             // X - e q is negative (add q) or at least q (subtract q): rare.
             if (live && (b0 || !b1)) {
                 uint32_t cb = 0;
-                for (int k = 0; k < L; ++k) {
-                    const uint32_t x = srow[k], qk = cc.q[k];
+                for (int kk = 0; kk < L; ++kk) {
+                    const uint32_t x = srow[kk], qk = cc.q[kk];
                     if (b0) {
                         const uint64_t sum = static_cast<uint64_t>(x) + qk + cb;
-                        srow[k] = static_cast<uint32_t>(sum);
+                        srow[kk] = static_cast<uint32_t>(sum);
                         cb = static_cast<uint32_t>(sum >> 32);
                     } else {
                         const uint64_t dd = static_cast<uint64_t>(x) - qk - cb;
-                        srow[k] = static_cast<uint32_t>(dd);
+                        srow[kk] = static_cast<uint32_t>(dd);
                         cb = static_cast<uint32_t>(dd >> 63);
                     }
                 }
             }
-            // The half's 128 rows are one contiguous run of c: copy it out
-            // with coalesced stores once every row is in outs.
-            tc::mbar_arrive(&sm.o_ready[h]);
-            ok = wait_or_abort(&sm.o_ready[h], it & 1, sm.abort);
+            // The tile's rows are one contiguous run of c: copy it out with
+            // coalesced stores once every row of the group is staged.
+            tc::mbar_arrive(&sm.o_sync[grp]);
+            ok = tc::wait_or_abort(&sm.o_sync[grp], 0, sm.abort, lim);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) break;
             {
-                const int rows_h = max(0, min(128, static_cast<int>(min(kSuper, n_end - n0)) - static_cast<int>(128 * h)));
-                uint32_t* gbase = C + static_cast<size_t>(n0 + 128 * h) * L;
-                const uint32_t* sbase = sm.outs + h * 128 * ostride;
+                uint32_t* gbase = C + static_cast<size_t>(n0) * L;
                 if (gvec) {
-                    const int q4 = L / 4, n4 = rows_h * q4;
-                    for (int i4 = static_cast<int>(hrow); i4 < n4; i4 += 128) {
+                    const int q4 = L / 4, n4 = static_cast<int>(rows_t) * q4;
+                    for (int i4 = static_cast<int>(row); i4 < n4; i4 += kCrtTile) {
                         const int r = i4 / q4, c4 = i4 - r * q4;
                         *reinterpret_cast<uint4*>(gbase + 4 * i4) =
-                            *reinterpret_cast<const uint4*>(sbase + r * ostride + 4 * c4);
+                            *reinterpret_cast<const uint4*>(obase + r * ostride + 4 * c4);
                     }
                 } else {
-                    const int nw = rows_h * L;
-                    for (int i = static_cast<int>(hrow); i < nw; i += 128) {
+                    const int nw = static_cast<int>(rows_t) * L;
+                    for (int i = static_cast<int>(row); i < nw; i += kCrtTile) {
                         const int r = i / L;
-                        gbase[i] = sbase[r * ostride + (i - r * L)];
+                        gbase[i] = obase[r * ostride + (i - r * L)];
                     }
                 }
             }
-            tc::mbar_arrive(&sm.o_free[h]);
+            // The staged rows may be overwritten once every thread has copied.
+            tc::mbar_arrive(&sm.o_sync[grp]);
+            ok = tc::wait_or_abort(&sm.o_sync[grp], 1, sm.abort, lim);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) break;
         }
     }
 
@@ -501,9 +522,10 @@ CrtConsts make_crt_consts(const HostPlan& pl) {
 }
 
 bool crt_pipe_supported(const DevPoint& d, const uint32_t* Y, uint32_t n_begin, uint32_t n_end) {
-    // Bulk copies of y rows need 16-byte aligned starts and lengths.
-    return d.L >= 2 && d.crt_u <= 256 && d.K + 1 <= kMaxK && d.crt_img_v && (d.N & 3) == 0 &&
-           (n_begin & 3) == 0 && (n_end & 3) == 0 && (reinterpret_cast<uintptr_t>(Y) & 15) == 0;
+    // TMA boxes of y: 16-byte aligned base, row pitch (N words) and column
+    // coordinates (n_begin) a multiple of 4 words.
+    return d.L >= 2 && d.crt_u <= 256 && d.K + 1 <= kMaxK && d.crt_img_v && (d.N & 3) == 0 && d.N >= kCrtTile &&
+           (n_begin & 3) == 0 && n_end <= d.N && (reinterpret_cast<uintptr_t>(Y) & 15) == 0;
 }
 
 void crt_pipe_init_attributes() {
@@ -517,15 +539,17 @@ void crt_pipe_init_attributes() {
 void launch_crt_pipe(const DevPoint& d, const CrtConsts& cc, const uint32_t* Y, uint32_t* c, uint32_t n_begin,
                      uint32_t n_end, int sms, cudaStream_t st) {
     if (n_end <= n_begin) return;
-    const uint32_t tiles = (n_end - n_begin + kSuper - 1) / kSuper;
+    const uint32_t tiles = (n_end - n_begin + kCrtTile - 1) / kCrtTile;
     const uint32_t grid = tiles < static_cast<uint32_t>(sms) ? tiles : static_cast<uint32_t>(sms);
+    // y: K rows of N words, boxes of 32 primes x 128 coefficients.
+    const CUtensorMap tm = make_tmap_u32(Y, static_cast<uint64_t>(d.K), d.N, d.N, kChunk, kCrtTile, TmaSwizzle::kNone);
     cudaError_t e = cudaSuccess;
     switch (d.L) {
-        case 64: e = launch_pdl(k_crt_pipe<64>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, Y, c, n_begin, n_end); break;
-        case 55: e = launch_pdl(k_crt_pipe<55>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, Y, c, n_begin, n_end); break;
-        case 28: e = launch_pdl(k_crt_pipe<28>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, Y, c, n_begin, n_end); break;
-        case 8: e = launch_pdl(k_crt_pipe<8>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, Y, c, n_begin, n_end); break;
-        default: e = launch_pdl(k_crt_pipe<0>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, Y, c, n_begin, n_end); break;
+        case 64: e = launch_pdl(k_crt_pipe<64>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, tm, c, n_begin, n_end); break;
+        case 55: e = launch_pdl(k_crt_pipe<55>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, tm, c, n_begin, n_end); break;
+        case 28: e = launch_pdl(k_crt_pipe<28>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, tm, c, n_begin, n_end); break;
+        case 8: e = launch_pdl(k_crt_pipe<8>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, tm, c, n_begin, n_end); break;
+        default: e = launch_pdl(k_crt_pipe<0>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, tm, c, n_begin, n_end); break;
     }
     check(e, "crt launch");
 }

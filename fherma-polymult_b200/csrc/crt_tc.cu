@@ -119,7 +119,7 @@ __device__ __forceinline__ void crt_body(const DevPoint& d, const uint32_t* __re
             const uint32_t idesc = tc::idesc_u8(U);
             for (int c = 0; c < nch && ok; ++c) {
                 const int s = c & 1;
-                ok = tc::wait_parity(&sm.b_full[s], (c >> 1) & 1) && tc::wait_parity(&sm.a_full[s], (c >> 1) & 1);
+                ok = tc::wait_parity(&sm.b_full[s], (c >> 1) & 1, d.wait_ns) && tc::wait_parity(&sm.a_full[s], (c >> 1) & 1, d.wait_ns);
                 if (!ok) break;
                 tc::tc_fence_after();
                 const uint32_t a0 = tc::smem_addr(sm.a0 + s * kASlot), b0 = tc::smem_addr(sm.b0 + s * chunk_bytes);
@@ -131,7 +131,7 @@ __device__ __forceinline__ void crt_body(const DevPoint& d, const uint32_t* __re
                 tc::mma_commit(&sm.mma_done[s]);
                 if (c >= 1 && c + 1 < nch) {
                     const int s1 = (c - 1) & 1;
-                    ok = tc::wait_parity(&sm.mma_done[s1], ((c - 1) >> 1) & 1);
+                    ok = tc::wait_parity(&sm.mma_done[s1], ((c - 1) >> 1) & 1, d.wait_ns);
                     if (!ok) break;
                     tc::mbar_arrive_expect_tx(&sm.b_full[s1], chunk_bytes);
                     tc::bulk_g2s(sm.b0 + s1 * chunk_bytes, d.crt_img + static_cast<size_t>(c + 1) * chunk_bytes, chunk_bytes,
@@ -150,7 +150,7 @@ __device__ __forceinline__ void crt_body(const DevPoint& d, const uint32_t* __re
         for (int c = 0; c < nch; ++c) {
             const int s = c & 1;
             if (c >= 2) {
-                ok = tc::wait_parity(&sm.mma_done[s], ((c - 2) >> 1) & 1);
+                ok = tc::wait_parity(&sm.mma_done[s], ((c - 2) >> 1) & 1, d.wait_ns);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
             }
@@ -180,7 +180,7 @@ __device__ __forceinline__ void crt_body(const DevPoint& d, const uint32_t* __re
             tc::mbar_arrive(&sm.a_full[s]);
         }
         if (ok) {
-            ok = tc::wait_parity(sm.d_ready, 0);
+            ok = tc::wait_parity(sm.d_ready, 0, d.wait_ns);
             ok = __all_sync(0xffffffffu, ok);
         }
         if (ok) {

@@ -12,18 +12,19 @@
 //     resident in shared memory) and then, one thread, issues the MMAs at the
 //     widest shape (N = 256 columns per chunk): D goes to one of two
 //     256-column TMEM buffers;
-//   * warps 1-4 stage the next tile's limbs into a two-slot ring in the MMA's
-//     K-major layout while the current tile is multiplied and folded: a warp
-//     moves 8 rows x 4 sixteen-byte groups at a time, so the global loads are
-//     64-byte runs and the eight lanes of each shared-store phase hit eight
-//     different bank groups;
+//   * warps 1-4 copy each tile's limbs into a two-slot ring in the MMA's
+//     K-major layout with asynchronous copies (cp.async), one tile in flight
+//     while the previous one lands and is multiplied: a warp moves 8 rows x 4
+//     sixteen-byte groups at a time, so the global loads are 64-byte runs and
+//     the eight lanes of each shared-store phase hit eight different bank
+//     groups;
 //   * warps 5-20, four per TMEM lane quadrant, one coefficient per thread,
 //     each take 16 of a chunk's 64 primes: read D, fold the 49-bit sums mod
 //     p_j and store the residues (a warp writes 32 consecutive words per
 //     prime).
-// The fold constants come from kernel parameters.  Every wait is bounded; a
-// timeout raises an abort flag that every role checks, and the error word gets
-// bit 0.
+// The fold constants come from kernel parameters.  Every wait is bounded
+// (DevPoint::wait_ns); a timeout raises an abort flag that every role checks,
+// and the error word gets bit 0.
 #include "device.cuh"
 #include "kernels.h"
 #include "pdl.cuh"
@@ -77,17 +78,22 @@ __device__ inline Smem carve(uint8_t* base, uint32_t kb, int nch, uint32_t nlast
     return s;
 }
 
-__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile uint32_t* abort) {
-    if (tc::mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = tc::globaltimer();
-    while (!tc::mbar_try_wait_sleep(bar, parity)) {
-        if (*abort) return false;
-        if (tc::globaltimer() - t0 > tc::kWaitNs) {
-            *abort = 1;
-            return false;
-        }
-    }
-    return true;
+// Asynchronous global -> shared copies of 16 or 4 bytes; with have == false
+// nothing is read and the destination is zero-filled.
+__device__ __forceinline__ void cp_async16_zfill(void* dst, const void* src, bool have) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(tc::smem_addr(dst)), "l"(src),
+                 "r"(have ? 16u : 0u)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4_zfill(void* dst, const void* src, bool have) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(tc::smem_addr(dst)), "l"(src),
+                 "r"(have ? 4u : 0u)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
 // A GEMM sum D is below 4L 255^2 <= 256 * 65025 (L <= 64), so both halves of
@@ -128,6 +134,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint32_t g0 = second ? split : 0, gs = second ? gridDim.x - split : split;
     const uint32_t tiles = (n_end - n_begin + kRows - 1) / kRows;
     const uint32_t chunk_bytes = kCols * kb;
+    const uint64_t lim = d.wait_ns;
 
     if (threadIdx.x == 0) {
         tc::mbar_init(sm.b_full, 1);
@@ -143,11 +150,15 @@ __global__ void __launch_bounds__(kThreads, 1)
         tc::fence_mbar_init();
         // The constant image is read-only plan data: it loads under the
         // preceding kernel's tail.
+        // (Test hook: with kFaultDecompose the image is never requested, so the
+        // MMA issuer's wait for it runs out.)
         const uint32_t total = static_cast<uint32_t>(b_bytes(kb, nch, nlast));
-        tc::mbar_arrive_expect_tx(sm.b_full, total);
-        for (uint32_t off = 0; off < total; off += chunk_bytes) {
-            const uint32_t n = total - off < chunk_bytes ? total - off : chunk_bytes;
-            tc::bulk_g2s(sm.b + off, img + off, n, sm.b_full);
+        if (!(d.fault & kFaultDecompose)) {
+            tc::mbar_arrive_expect_tx(sm.b_full, total);
+            for (uint32_t off = 0; off < total; off += chunk_bytes) {
+                const uint32_t n = total - off < chunk_bytes ? total - off : chunk_bytes;
+                tc::bulk_g2s(sm.b + off, img + off, n, sm.b_full);
+            }
         }
     }
     if (warp == 0) tc::tmem_alloc(sm.tmem_base, 512);
@@ -161,19 +172,19 @@ __global__ void __launch_bounds__(kThreads, 1)
         // ---- MMA issuer ----
         if (lane == 0) {
             const uint32_t idesc_full = tc::idesc_u8(kCols), idesc_last = tc::idesc_u8(nlast);
-            bool ok = wait_or_abort(sm.b_full, 0, sm.abort);
+            bool ok = tc::wait_or_abort(sm.b_full, 0, sm.abort, lim);
             uint64_t* last_bar = nullptr;   // the barrier of the latest commit
             uint32_t last_par = 0;
             uint32_t g = 0, i = 0;
             for (uint32_t t = blockIdx.x - g0; ok && t < tiles; t += gs, ++i) {
                 const int s = i & 1;
-                ok = wait_or_abort(&sm.a_full[s], (i >> 1) & 1, sm.abort);
+                ok = tc::wait_or_abort(&sm.a_full[s], (i >> 1) & 1, sm.abort, lim);
                 if (!ok) break;
                 const uint32_t a0 = tc::smem_addr(sm.a + s * a_bytes(kb));
                 for (int c = 0; c < nch; ++c, ++g) {
                     const int buf = g & 1;
                     if (g >= 2) {
-                        ok = wait_or_abort(&sm.d_empty[buf], ((g - 2) >> 1) & 1, sm.abort);
+                        ok = tc::wait_or_abort(&sm.d_empty[buf], ((g - 2) >> 1) & 1, sm.abort, lim);
                         if (!ok) break;
                     }
                     tc::tc_fence_after();
@@ -195,59 +206,70 @@ __global__ void __launch_bounds__(kThreads, 1)
                 last_par = (i >> 1) & 1;
             }
             // MMAs still running must finish before the CTA may exit.
-            if (last_bar) tc::wait_parity(last_bar, last_par);
+            if (last_bar) tc::wait_parity(last_bar, last_par, lim);
+            // So must the constant image, if an abort came before it landed.
+            if (!(d.fault & kFaultDecompose)) tc::wait_parity(sm.b_full, 0, lim);
         }
         __syncwarp();
     } else if (warp < kEpiWarp0) {
-        // ---- loaders: the next tile's limbs, K-major with a padded K stride ----
-        const uint32_t lt = threadIdx.x - kLoadWarp0 * 32;
+        // ---- loaders: each tile's limbs, K-major with a padded K stride ----
+        // The copies go from global to shared memory asynchronously (cp.async,
+        // zero-filled where a position has no limb: rows past nk, limbs past
+        // L), so one whole tile is in flight while the previous one completes.
+        // A warp covers an 8-row x 4-group block per instruction: every lane
+        // group of a shared-store phase hits distinct banks.
+        const uint32_t lt = threadIdx.x - kLoadWarp0 * 32, lw = lt >> 5;
         const bool vec = (reinterpret_cast<uintptr_t>(limbs) & 15u) == 0 && (L & 3) == 0;
-        const uint32_t kw = kb / 4;
+        const uint32_t G = kb / 16;                    // 16-byte K groups per row
+        const uint32_t r = lane & 7, gi = lane >> 3;   // row in block, group (or limb) in block
+        const uint32_t gbs = (G + 3) / 4;
         uint32_t i = 0;
+        bool ok = true;
         for (uint32_t t = blockIdx.x - g0; t < tiles; t += gs, ++i) {
             const int s = i & 1;
             if (i >= 2) {
-                bool ok = wait_or_abort(&sm.a_empty[s], ((i - 2) >> 1) & 1, sm.abort);
+                ok = tc::wait_or_abort(&sm.a_empty[s], ((i - 2) >> 1) & 1, sm.abort, lim);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
             }
             uint8_t* at = sm.a + s * a_bytes(kb);
             const uint32_t n0 = n_begin + t * kRows;
             const uint32_t nk = min(kRows, n_end - n0);
-            // Every position of the tile is written once: a limb, or zero for
-            // rows past nk and limbs past L.
             if (vec) {
-                // 16-byte group gq of row m is limbs 4 gq .. 4 gq + 3; block
-                // (mb, gb) is rows 8 mb .. + 7 and groups 4 gb .. + 3.
-                const uint32_t q4 = static_cast<uint32_t>(L) / 4, G = kb / 16, gbs = (G + 3) / 4;
-                const uint32_t nblk = (kRows / 8) * gbs, lw = lt >> 5;
-                const uint32_t r = lane & 7, gi = lane >> 3;
+                // Block (mb, gb): rows 8 mb .. + 7, 16-byte groups 4 gb .. + 3
+                // (group gq of a row is limbs 4 gq .. 4 gq + 3).
+                const uint32_t q4 = static_cast<uint32_t>(L) / 4;
                 const uint4* src4 = reinterpret_cast<const uint4*>(limbs + static_cast<size_t>(n0) * L);
-                for (uint32_t b0 = lw; b0 < nblk; b0 += 8 * (kLoaders / 32)) {
-                    uint4 v[8];
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const uint32_t blk = b0 + k * (kLoaders / 32), mb = blk / gbs, gb = blk - mb * gbs;
-                        const uint32_t mm = 8 * mb + r, gq = 4 * gb + gi;
-                        v[k] = (blk < nblk && mm < nk && gq < q4) ? __ldg(src4 + mm * q4 + gq) : make_uint4(0, 0, 0, 0);
-                    }
-#pragma unroll
-                    for (int k = 0; k < 8; ++k) {
-                        const uint32_t blk = b0 + k * (kLoaders / 32), mb = blk / gbs, gb = blk - mb * gbs;
-                        const uint32_t mm = 8 * mb + r, gq = 4 * gb + gi;
-                        if (blk < nblk && gq < G) *reinterpret_cast<uint4*>(at + gq * kALbo + mm * 16) = v[k];
+                for (uint32_t blk = lw; blk < 16 * gbs; blk += kLoaders / 32) {
+                    const uint32_t mm = 8 * (blk & 15) + r, gq = 4 * (blk >> 4) + gi;
+                    if (gq < G) {
+                        const bool have = mm < nk && gq < q4;
+                        cp_async16_zfill(at + gq * kALbo + mm * 16, have ? src4 + mm * q4 + gq : src4, have);
                     }
                 }
             } else {
+                // Block (mb, gq): rows 8 mb .. + 7, limbs 4 gq .. 4 gq + 3.
                 const uint32_t* src = limbs + static_cast<size_t>(n0) * L;
-                for (uint32_t w = lt; w < kRows * kw; w += kLoaders) {
-                    const uint32_t mm = w / kw, l = w - mm * kw;
-                    const uint32_t v = (mm < nk && l < static_cast<uint32_t>(L)) ? src[mm * L + l] : 0u;
-                    *reinterpret_cast<uint32_t*>(at + (l >> 2) * kALbo + mm * 16 + (l & 3) * 4) = v;
+                for (uint32_t blk = lw; blk < 16 * G; blk += kLoaders / 32) {
+                    const uint32_t mm = 8 * (blk & 15) + r, l = 4 * (blk >> 4) + gi;
+                    const bool have = mm < nk && l < static_cast<uint32_t>(L);
+                    cp_async4_zfill(at + (l >> 2) * kALbo + mm * 16 + (l & 3) * 4,
+                                    have ? src + mm * L + l : src, have);
                 }
             }
+            cp_async_commit();
+            if (i >= 1) {
+                // The previous tile's copies have landed: hand it to the MMAs.
+                cp_async_wait<1>();
+                tc::fence_proxy_async_smem();
+                tc::mbar_arrive(&sm.a_full[s ^ 1]);
+            }
+        }
+        // The last tile (and, after an abort, whatever is still in flight).
+        cp_async_wait<0>();
+        if (ok && i >= 1) {
             tc::fence_proxy_async_smem();
-            tc::mbar_arrive(&sm.a_full[s]);
+            tc::mbar_arrive(&sm.a_full[(i - 1) & 1]);
         }
     } else {
         // ---- epilogue: thread = one coefficient, 16 primes of each chunk ----
@@ -262,7 +284,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             bool ok = true;
             for (int c = 0; c < nch; ++c, ++g) {
                 const int buf = g & 1;
-                ok = wait_or_abort(&sm.d_full[buf], (g >> 1) & 1, sm.abort);
+                ok = tc::wait_or_abort(&sm.d_full[buf], (g >> 1) & 1, sm.abort, lim);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
                 tc::tc_fence_after();

@@ -166,8 +166,8 @@ __device__ __forceinline__ void dec_body(const DevPoint& d, const uint32_t* __re
             const uint32_t a0 = tc::smem_addr(sm.a);
             for (int c = 0; c < nch && ok; ++c) {
                 const int s = c & 1;
-                ok = tc::wait_parity(&sm.full[s], (c >> 1) & 1);
-                if (ok && c >= 2) ok = tc::wait_parity(&sm.tmem_empty[s], ((c - 2) >> 1) & 1);
+                ok = tc::wait_parity(&sm.full[s], (c >> 1) & 1, d.wait_ns);
+                if (ok && c >= 2) ok = tc::wait_parity(&sm.tmem_empty[s], ((c - 2) >> 1) & 1, d.wait_ns);
                 if (!ok) break;
                 tc::tc_fence_after();
                 const uint32_t b0 = tc::smem_addr(sm.b0 + s * chunk_bytes);
@@ -179,7 +179,7 @@ __device__ __forceinline__ void dec_body(const DevPoint& d, const uint32_t* __re
                 tc::mma_commit(&sm.mma_done[s]);
                 if (c >= 1 && c + 1 < nch) {
                     const int s1 = (c - 1) & 1;
-                    ok = tc::wait_parity(&sm.mma_done[s1], ((c - 1) >> 1) & 1);
+                    ok = tc::wait_parity(&sm.mma_done[s1], ((c - 1) >> 1) & 1, d.wait_ns);
                     if (!ok) break;
                     tc::mbar_arrive_expect_tx(&sm.full[s1], chunk_bytes);
                     tc::bulk_g2s(sm.b0 + s1 * chunk_bytes, img + static_cast<size_t>(c + 1) * chunk_bytes, chunk_bytes,
@@ -189,7 +189,7 @@ __device__ __forceinline__ void dec_body(const DevPoint& d, const uint32_t* __re
             if (ok) {
                 // The last MMAs must finish before the block can release TMEM.
                 const int c = nch - 1;
-                ok = tc::wait_parity(&sm.mma_done[c & 1], (c >> 1) & 1);
+                ok = tc::wait_parity(&sm.mma_done[c & 1], (c >> 1) & 1, d.wait_ns);
             }
         }
         __syncwarp();
@@ -200,7 +200,7 @@ __device__ __forceinline__ void dec_body(const DevPoint& d, const uint32_t* __re
         const uint32_t tq = tmem + ((q * 32) << 16);
         for (int c = 0; c < nch; ++c) {
             const int s = c & 1;
-            ok = tc::wait_parity(&sm.mma_done[s], (c >> 1) & 1);
+            ok = tc::wait_parity(&sm.mma_done[s], (c >> 1) & 1, d.wait_ns);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) break;
             tc::tc_fence_after();

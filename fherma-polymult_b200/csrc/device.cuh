@@ -43,6 +43,18 @@ struct DevPoint {
     uint32_t negp_top;         // (-P mod q)'s top limb
     // error word: bit 0 decompose, bit 1 CRT (a pipeline wait timed out)
     uint32_t* err;
+    // How long any pipeline wait may last before the kernel gives up, sets the
+    // error word and returns (nanoseconds; 2 s unless a caller shortens it).
+    uint64_t wait_ns;
+    // Test hook, 0 in every product: bit 0 makes the pipelined decompose, bit 1
+    // the pipelined CRT, leave one barrier phase that a role waits on without
+    // its arrival, so that wait runs out (kFault* below).
+    uint32_t fault;
+};
+
+enum FaultBits : uint32_t {
+    kFaultDecompose = 1u,
+    kFaultCrt = 2u,
 };
 
 // What the row kernel does with its tile.

@@ -89,6 +89,8 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
         dp_.crt_img = upload(pl.crt_img);
         dp_.crt_img_v = upload(pl.crt_img_v);
         dp_.negp_top = pl.negp_top;
+        dp_.wait_ns = kDefaultWaitNs;
+        dp_.fault = 0;
         if (crt_uses_tc(pl)) crt_consts_.reset(new CrtConsts(make_crt_consts(pl)));
         if (decompose_pipe_supported(pl)) {
             const uint8_t* wa = upload(pl.dec_wimg_a);
@@ -147,13 +149,14 @@ void Engine::launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, u
     }
 }
 
-void Engine::launch_crt_any(const uint32_t* d_y, uint32_t* d_c, uint32_t n0, uint32_t n1, cudaStream_t st) {
+void Engine::launch_crt_any(const DevPoint& d, const uint32_t* d_y, uint32_t* d_c, uint32_t n0, uint32_t n1,
+                            cudaStream_t st) {
     if (simt_ || !crt_uses_tc(plan_)) {
-        launch_crt(dp_, d_y, d_c, n0, n1, st);
-    } else if (crt_consts_ && crt_pipe_supported(dp_, d_y, n0, n1)) {
-        launch_crt_pipe(dp_, *crt_consts_, d_y, d_c, n0, n1, sms_, st);
+        launch_crt(d, d_y, d_c, n0, n1, st);
+    } else if (crt_consts_ && crt_pipe_supported(d, d_y, n0, n1)) {
+        launch_crt_pipe(d, *crt_consts_, d_y, d_c, n0, n1, sms_, st);
     } else {
-        launch_crt_tc(dp_, d_y, d_c, n0, n1, st);
+        launch_crt_tc(d, d_y, d_c, n0, n1, st);
     }
 }
 
@@ -162,6 +165,11 @@ uint32_t Engine::take_error() {
     check(cudaMemcpy(&e, dp_.err, sizeof(e), cudaMemcpyDeviceToHost), "read error word");
     if (e) check(cudaMemset(dp_.err, 0, sizeof(e)), "clear error word");
     return e;
+}
+
+uint32_t Engine::take_error(cudaStream_t st) {
+    check(cudaStreamSynchronize(st), "stream synchronize");
+    return take_error();
 }
 
 void Engine::decompose(const uint32_t* d_limbs, uint32_t* d_res, int operand, cudaStream_t st) {
@@ -175,22 +183,28 @@ void Engine::transform(uint32_t* d_A, uint32_t* d_B, int mode, cudaStream_t st) 
 }
 
 void Engine::crt(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st) {
-    launch_crt_any(d_y, d_c, 0, plan_.N, st);
+    launch_crt_any(dp_, d_y, d_c, 0, plan_.N, st);
     check(cudaGetLastError(), "crt launch");
 }
 
-void Engine::run_device(const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t st) {
+void Engine::product(const DevPoint& d, const uint32_t* d_a, const uint32_t* d_b, uint32_t* A, uint32_t* B,
+                     uint32_t* d_c, cudaStream_t st) {
+    const uint32_t N = plan_.N;
     if (simt_) {
-        launch_dec(d_a, A_, 0, 0, plan_.N, st);
-        launch_dec(d_b, B_, 1, 0, plan_.N, st);
+        launch_decompose(d, d_a, A, 0, 0, N, st);
+        launch_decompose(d, d_b, B, 1, 0, N, st);
     } else if (dec_consts_) {
-        launch_decompose_pipe(dp_, *dec_consts_, d_a, d_b, A_, B_, 0, 0, plan_.N, sms_, st);
+        launch_decompose_pipe(d, *dec_consts_, d_a, d_b, A, B, 0, 0, N, sms_, st);
     } else {
-        launch_decompose_tc_pair(dp_, d_a, d_b, A_, B_, st);
+        launch_decompose_tc_pair(d, d_a, d_b, A, B, st);
     }
-    launch_ntt(dp_, A_, B_, kRowProduct, st);
-    launch_crt_any(A_, d_c, 0, plan_.N, st);
+    launch_ntt(d, A, B, kRowProduct, st);
+    launch_crt_any(d, A, d_c, 0, N, st);
     check(cudaGetLastError(), "product launch");
+}
+
+void Engine::run_device(const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t st) {
+    product(dp_, d_a, d_b, A_, B_, d_c, st);
 }
 
 namespace {
@@ -273,7 +287,7 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_
     for (size_t k = 0; k < nch; ++k) {
         const uint32_t n0 = chunk_at_[k], n1 = chunk_at_[k + 1];
         const size_t off = static_cast<size_t>(n0) * L, bytes = static_cast<size_t>(n1 - n0) * L * 4;
-        launch_crt_any(A_, lc_, n0, n1, stream_);
+        launch_crt_any(dp_, A_, lc_, n0, n1, stream_);
         check(cudaEventRecord(crt_ev[k], stream_), "event");
         check(cudaStreamWaitEvent(out_, crt_ev[k], 0), "wait");
         check(cudaMemcpyAsync(dst + off, lc_ + off, bytes, cudaMemcpyDeviceToHost, out_), "copy out");
@@ -292,7 +306,8 @@ void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_
         check(cudaEventSynchronize(out_ev[nch - 1]), "copy out");
     }
     if (const uint32_t e = take_error()) {
-        throw std::runtime_error("a kernel pipeline wait timed out (error word " + std::to_string(e) + ")");
+        throw PipelineTimeout("a kernel pipeline wait ran out of time (error word " + std::to_string(e) +
+                              "); this product's result is not valid");
     }
 }
 

@@ -65,16 +65,33 @@ public:
     // Reads and clears the device error word (nonzero: a pipeline wait in a
     // tensor-core kernel timed out); synchronous.
     uint32_t take_error();
+    // The same after waiting for the work enqueued on st.
+    uint32_t take_error(cudaStream_t st);
+    // Reads and clears the error word of the static scratch array on the
+    // current device (fpm_run_device_noalloc's calls), after waiting for st.
+    static uint32_t take_static_error(cudaStream_t st);
+
+    // Limit of every pipeline wait in this engine's kernels, in nanoseconds
+    // (DevPoint::wait_ns); applies to products enqueued afterwards.
+    void set_wait_limit(uint64_t ns) { dp_.wait_ns = ns; }
+    // Test hook (DevPoint::fault): the pipelines of products enqueued
+    // afterwards leave one barrier phase without its arrival.
+    void set_fault(uint32_t mask) { dp_.fault = mask; }
 
     size_t words() const { return static_cast<size_t>(plan_.N) * plan_.L; }
     size_t residues() const { return static_cast<size_t>(plan_.K) * plan_.N; }
 
 private:
     size_t static_scratch_err_offset() const;
+    // The product's launches on workspaces A, B with point d (whose err names
+    // the error word to use).
+    void product(const DevPoint& d, const uint32_t* d_a, const uint32_t* d_b, uint32_t* A, uint32_t* B, uint32_t* d_c,
+                 cudaStream_t st);
     void release();
     void launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, uint32_t n0, uint32_t n1,
                     cudaStream_t st);
-    void launch_crt_any(const uint32_t* d_y, uint32_t* d_c, uint32_t n0, uint32_t n1, cudaStream_t st);
+    void launch_crt_any(const DevPoint& d, const uint32_t* d_y, uint32_t* d_c, uint32_t n0, uint32_t n1,
+                        cudaStream_t st);
     void ensure_host_path();
     template <class T>
     T* dalloc(size_t count);

@@ -18,9 +18,18 @@ struct CudaError : std::runtime_error {
     CudaError(const std::string& msg, cudaError_t c) : std::runtime_error(msg), code(c) {}
 };
 
+// A pipeline wait in a tensor-core kernel ran out of time (DevPoint::wait_ns):
+// the kernel returned early and that product's result is wrong.
+struct PipelineTimeout : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
 inline void check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) throw CudaError(std::string(what) + ": " + cudaGetErrorString(e), e);
 }
+
+// Default limit of a pipeline wait (DevPoint::wait_ns): 2 s.
+constexpr uint64_t kDefaultWaitNs = 2000000000ull;
 
 // Columns per column-pass tile of 2048 elements.
 template <int LOGR>

@@ -13,7 +13,8 @@
 //     vector loads; the row pass's tables are stored round-major, so those
 //     loads are free of bank conflicts;
 //   * the row pass uses only the FORWARD twiddle tables of its rows (prebuilt
-//     once per context from two small per-prime tables), and pairs row u with
+//     once per context from two small per-prime tables and brought into
+//     shared memory by bulk asynchronous copies), and pairs row u with
 //     row R - 1 - u: the inverse
 //     twiddle of row u at entry y is minus the forward twiddle of row R - 1 - u
 //     at y with its low bits complemented (psi^(N - e) = -psi^-e), so one
@@ -25,6 +26,7 @@
 #include "kernels.h"
 #include "ntt_engine.cuh"
 #include "pdl.cuh"
+#include "tc.cuh"
 
 #include <type_traits>
 
@@ -73,14 +75,6 @@ __device__ __forceinline__ void inv_range(uint32_t* tile, const TW& tw, uint32_t
         inv_range<NSUB, XS, SWZ, RB, R - 1, RLO, LAZY, NEG>(tile, tw, p);
     }
 }
-
-// 16-byte asynchronous global -> shared copies (both addresses 16-byte aligned).
-__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src) {
-    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst_smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Canonical residue from a lazy one (< 4p).
 __device__ __forceinline__ uint32_t canon4(uint32_t x, uint32_t p) {
@@ -246,23 +240,22 @@ __device__ __forceinline__ uint32_t row_of_slot(uint32_t slot, uint32_t u0, uint
 }
 
 // Copies the block's row tables (slot s holds row row_of_slot(s)) from the
-// prebuilt K x R x S array into shared memory with 16-byte asynchronous copies;
-// the caller waits with cp_async_wait_all() before its barrier.
-template <int LOGS, int T>
-__device__ __forceinline__ void row_tables_async(uint2* tf, const DevPoint& d, int j, uint32_t u0) {
+// prebuilt K x R x S array into shared memory with bulk asynchronous copies
+// (one per row table, S Shoup pairs, issued by the lanes of warp 0), counted
+// on the mbarrier `bar`, which the caller waits on (phase parity `phase`)
+// before its first twiddle read.  Called by warp 0 only.
+template <int LOGS>
+__device__ __forceinline__ void row_tables_bulk(uint2* tf, const DevPoint& d, int j, uint32_t u0, uint64_t* bar) {
     using RG = RowGeom<LOGS>;
     const uint32_t R = 1u << d.logR;
-    constexpr uint32_t kChunks = RG::kSlots * RG::S / 2;   // 16-byte pairs
-    static_assert(kChunks % T == 0, "whole chunks per thread");
-#pragma unroll
-    for (uint32_t t = 0; t < kChunks / T; ++t) {
-        const uint32_t c = threadIdx.x + t * T;
-        const uint32_t slot = c / (RG::S / 2), y = 2 * (c % (RG::S / 2));
+    constexpr uint32_t kBytes = RG::S * sizeof(uint2);
+    const int lane = threadIdx.x & 31;
+    if (lane == 0) tc::mbar_arrive_expect_tx(bar, RG::kSlots * kBytes);
+    __syncwarp();
+    for (uint32_t slot = lane; slot < RG::kSlots; slot += 32) {
         const uint32_t u = row_of_slot<LOGS>(slot, u0, R);
-        const uint2* src = d.row_tw + (static_cast<size_t>(j) * R + u) * RG::S + y;
-        cp_async16(tf + slot * RG::kStride + y, src);
+        tc::bulk_g2s(tf + slot * RG::kStride, d.row_tw + (static_cast<size_t>(j) * R + u) * RG::S, kBytes, bar);
     }
-    cp_async_commit();
 }
 
 // One row's forward table, position p (round-major): U[u][b(p)] Q'[p] with its
@@ -291,8 +284,17 @@ __device__ __forceinline__ size_t row_offset(uint32_t i, uint32_t u0, uint32_t R
     return static_cast<size_t>(row_of_slot<LOGS>(i >> LOGS, u0, R)) * (1u << LOGS) + (i & ((1u << LOGS) - 1u));
 }
 
+// The row pass's tables barrier sits after the tiles and the tables.
+template <int LOGS>
+constexpr size_t row_bar_offset() {
+    return 2 * 2048 * sizeof(uint32_t) + RowGeom<LOGS>::kSlots * RowGeom<LOGS>::kStride * sizeof(uint2);
+}
+
+// phase: parity of this tile's use of the tables barrier (the block's tile
+// count so far, mod 2); the barrier is initialised by the kernel.
 template <int LOGS, bool LAZY>
-__device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, int j, uint32_t bx) {
+__device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, int j, uint32_t bx,
+                                         uint32_t phase) {
     extern __shared__ __align__(1024) uint32_t smem[];
     using RG = RowGeom<LOGS>;
     constexpr int RB = row_pass_rb(LOGS), E = 1 << RB, T = ntt_threads<RB>();
@@ -312,8 +314,9 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
     const RowTable<LOGS, RG::kStride, true, RG::kFlip> iw{tf};
     uint32_t* const tiles[2] = {ta, tb};
 
+    uint64_t* tbar = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(smem) + row_bar_offset<LOGS>());
     // The tables stream into shared memory while round 0 loads its elements.
-    row_tables_async<LOGS, T>(tf, d, j, u0);
+    if (threadIdx.x < 32) row_tables_bulk<LOGS>(tf, d, j, u0, tbar);
     // Round 0 straight from global memory (the thread's E elements lie in one row).
     {
         const uint32_t base = round_base<LOGS, 0, SwzRow, RB, 0>(threadIdx.x);
@@ -325,8 +328,9 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
             v[0][k] = a[at + (k << sh)];
             v[1][k] = b[at + (k << sh)];
         }
-        cp_async_wait_all();
-        __syncthreads();
+        // The bound only guards against a copy that never lands: past it the
+        // error word gets bit 2 and the block goes on (with wrong twiddles).
+        if (!tc::wait_parity(tbar, phase, d.wait_ns) && (threadIdx.x & 31) == 0) atomicOr(d.err, 4u);
         fwd_round<LOGS, 0, SwzRow, RB, 0, LAZY, 2>(v, base, fw, p);
 #pragma unroll
         for (int o = 0; o < 2; ++o) store_round<LOGS, 0, SwzRow, RB, 0>(tiles[o], v[o], base);
@@ -446,9 +450,16 @@ __global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>(
 
 template <int LOGS, bool LAZY>
 __global__ void __launch_bounds__(row_threads<LOGS>(), (row_min_blocks<LOGS>())) k_ntt_row(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
+    extern __shared__ __align__(1024) uint32_t smem[];
+    uint64_t* tbar = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(smem) + row_bar_offset<LOGS>());
+    if (threadIdx.x == 0) {
+        tc::mbar_init(tbar, 1);
+        tc::fence_mbar_init();
+    }
+    __syncthreads();
     pdl_launch_dependents();
     pdl_wait();
-    row_body<LOGS, LAZY>(d, A, B, mode, blockIdx.y, blockIdx.x);
+    row_body<LOGS, LAZY>(d, A, B, mode, blockIdx.y, blockIdx.x, 0);
 }
 
 // Grouped launches over products of one geometry class: a (possibly
@@ -483,12 +494,20 @@ __global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>(
 
 template <int LOGS, bool LAZY>
 __global__ void __launch_bounds__(row_threads<LOGS>(), (row_min_blocks<LOGS>())) k_ntt_row_group(const __grid_constant__ GroupTable t) {
-    for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
+    extern __shared__ __align__(1024) uint32_t smem[];
+    uint64_t* tbar = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(smem) + row_bar_offset<LOGS>());
+    if (threadIdx.x == 0) {
+        tc::mbar_init(tbar, 1);
+        tc::fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t n = 0;
+    for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x, ++n) {
         if (b != blockIdx.x) __syncthreads();
         const uint32_t i = group_locate(t, b);
         const GroupItem& it = t.item[i];
         const uint32_t local = b - t.first[i], per = row_blocks<LOGS>(it.d.logR);
-        row_body<LOGS, LAZY>(it.d, it.A, it.B, kRowProduct, it.j0 + local / per, local % per);
+        row_body<LOGS, LAZY>(it.d, it.A, it.B, kRowProduct, it.j0 + local / per, local % per, n & 1);
     }
 }
 
@@ -545,7 +564,7 @@ size_t col_inv_smem_t(uint32_t logR) { return 2048 * sizeof(uint32_t) + (size_t(
 
 template <int LOGS>
 constexpr size_t row_smem_t() {
-    return 2 * 2048 * sizeof(uint32_t) + RowGeom<LOGS>::kSlots * RowGeom<LOGS>::kStride * sizeof(uint2);
+    return row_bar_offset<LOGS>() + 16;
 }
 
 template <int LOGR, int LOGS, bool LAZY>

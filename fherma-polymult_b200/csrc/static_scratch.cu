@@ -1,8 +1,8 @@
 // The product with its scratch in a static device array (fpm_run_device_noalloc).
 //
 // Some callers cannot call cudaMalloc once they are running: a process under a
-// fixed device-memory budget, or code that issues work where allocation is not
-// allowed (for example while a stream is being captured).  fpm_run_device
+// fixed device-memory budget that it may not grow, or a caller whose own rules
+// forbid allocating on its hot path.  fpm_run_device
 // itself allocates nothing either, but it uses the residue workspaces that
 // fpm_init allocated for its context.  This variant never touches those: the
 // product's scratch -- the two residue workspaces (2 K N words) and the
@@ -17,11 +17,22 @@
 // device does that lookup, which also loads this file's module; make that first
 // call before any stream capture.
 //
+// The kernels are the ones fpm_run_device launches (the pipelined decompose
+// and CRT where the point has them); their constants are the context's,
+// uploaded by fpm_init, and the CRT's tensor map is encoded on the host.
+//
 // Every call shares the array and it keeps the last call's contents: the
-// residue workspaces are fully rewritten by the decompose kernels, and the
-// error word is cleared at the start of each call.  Calls whose work overlaps
-// on the GPU (different streams, or different host threads without ordering)
-// race on the array; order them on one stream.
+// residue workspaces are fully rewritten by the decompose kernels.  The error
+// word is not cleared by a call: a kernel whose pipeline wait runs out sets a
+// bit in it, and the bit stays until fpm_noalloc_get_error reads and clears
+// it, so a caller that checks after a run of calls learns whether any of them
+// failed.  Calls whose work overlaps on the GPU (different streams, or
+// different host threads without ordering) race on the array; order them on
+// one stream.
+//
+// The address lookup is cached per device for the life of the process; after
+// cudaDeviceReset on a device the cached address is stale, so the library must
+// not be used on that device again in the same process.
 #include "engine.h"
 #include "kernels.h"
 
@@ -35,6 +46,7 @@ namespace {
 
 constexpr size_t kStaticScratchBytes = size_t(80) << 20;
 constexpr size_t kStaticScratchWords = kStaticScratchBytes / sizeof(uint32_t);
+constexpr size_t kStaticErrWord = kStaticScratchWords - 64;
 
 static __device__ __align__(256) uint32_t g_fpm_static_scratch[kStaticScratchWords];
 
@@ -58,10 +70,10 @@ void* scratch_address(int device) {
 
 size_t static_scratch_bytes() { return kStaticScratchBytes; }
 
-// Scratch layout in words: A and B (K N each), then the error word on its own
-// 256-byte line.
-size_t Engine::static_scratch_err_offset() const { return (2 * residues() + 63) / 64 * 64; }
-size_t Engine::static_scratch_words_needed() const { return static_scratch_err_offset() + 64; }
+// Scratch layout in words: A and B (K N each) from the start, the error word in
+// the array's last 256-byte line, the same for every point.
+size_t Engine::static_scratch_err_offset() const { return kStaticErrWord; }
+size_t Engine::static_scratch_words_needed() const { return (2 * residues() + 63) / 64 * 64 + 64; }
 
 void Engine::run_device_static(const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c, cudaStream_t st) {
     const size_t need = static_scratch_words_needed();
@@ -78,27 +90,22 @@ void Engine::run_device_static(const uint32_t* d_a, const uint32_t* d_b, uint32_
                                  " but device " + std::to_string(cur) + " is current");
     }
     uint32_t* base = static_cast<uint32_t*>(scratch_address(cur));
-    uint32_t* A = base;
-    uint32_t* B = base + residues();
-    uint32_t* err = base + static_scratch_err_offset();
-    check(cudaMemsetAsync(err, 0, sizeof(uint32_t), st), "clear error word");
     DevPoint d = dp_;
-    d.err = err;
-    const uint32_t N = plan_.N;
-    if (simt_) {
-        launch_decompose(d, d_a, A, 0, 0, N, st);
-        launch_decompose(d, d_b, B, 1, 0, N, st);
-    } else {
-        launch_decompose_tc(d, d_a, A, 0, 0, N, st);
-        launch_decompose_tc(d, d_b, B, 1, 0, N, st);
-    }
-    launch_ntt(d, A, B, kRowProduct, st);
-    if (simt_ || !crt_uses_tc(plan_)) {
-        launch_crt(d, A, d_c, 0, N, st);
-    } else {
-        launch_crt_tc(d, A, d_c, 0, N, st);
-    }
-    check(cudaGetLastError(), "product launch");
+    d.err = base + static_scratch_err_offset();
+    product(d, d_a, d_b, base, base + residues(), d_c, st);
+}
+
+uint32_t Engine::take_static_error(cudaStream_t st) {
+    int cur = -1;
+    check(cudaGetDevice(&cur), "cudaGetDevice");
+    // The error word sits at the same place for every point: right after the
+    // largest workspaces the array can hold.
+    uint32_t* err = static_cast<uint32_t*>(scratch_address(cur)) + kStaticErrWord;
+    check(cudaStreamSynchronize(st), "stream synchronize");
+    uint32_t e = 0;
+    check(cudaMemcpy(&e, err, sizeof(e), cudaMemcpyDeviceToHost), "read error word");
+    if (e) check(cudaMemset(err, 0, sizeof(e)), "clear error word");
+    return e;
 }
 
 }  // namespace fpm

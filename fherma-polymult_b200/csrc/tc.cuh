@@ -2,10 +2,12 @@
 // async copies, TMEM allocation, tcgen05.mma (kind::i8, one CTA), tcgen05.ld,
 // and UMMA shared-memory / instruction descriptors.
 //
-// Every wait is bounded: wait_parity() gives up after kWaitNs nanoseconds and
-// reports failure, so a kernel whose pipeline stalls sets an error word and
-// returns instead of hanging the GPU.
+// Every wait is bounded: wait_parity() gives up after a limit (kWaitNs unless
+// the caller passes one) and reports failure, so a kernel whose pipeline
+// stalls sets an error word and returns instead of hanging the GPU.
 #pragma once
+
+#include <cuda.h>
 
 #include <cstdint>
 
@@ -68,12 +70,29 @@ __device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t pari
     return ok != 0;
 }
 
-// Waits for the phase with the given parity to complete; false on timeout.
-__device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity) {
+// Waits for the phase with the given parity to complete; false after
+// limit_ns nanoseconds.
+__device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity, uint64_t limit_ns = kWaitNs) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer();
     while (!mbar_try_wait_sleep(bar, parity)) {
-        if (globaltimer() - t0 > kWaitNs) return false;
+        if (globaltimer() - t0 > limit_ns) return false;
+    }
+    return true;
+}
+
+// As wait_parity, but also gives up (false) once another role of the CTA has
+// raised *abort; a wait that runs out of time raises it.
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity, volatile uint32_t* abort,
+                                              uint64_t limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer();
+    while (!mbar_try_wait_sleep(bar, parity)) {
+        if (*abort) return false;
+        if (globaltimer() - t0 > limit_ns) {
+            *abort = 1;
+            return false;
+        }
     }
     return true;
 }
@@ -86,6 +105,37 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
             smem_addr(dst)),
         "l"(src), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
+}
+
+// 2-D tensor copies through a tensor map (tmap.h) of this GPU's memory.  x is
+// the column (word) coordinate, y the row; x * 4 bytes must be a multiple of
+// 16.  The map lives in kernel-parameter space (__grid_constant__).
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Shared -> global through a tensor map; the rows of the box at (x, y) that lie
+// inside the array are written.  Completion is tracked per thread with
+// bulk_commit / bulk_wait_read / bulk_wait_all.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void* src, int x, int y) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(smem_addr(src))
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// The source shared memory of every committed store may be reused.
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// Every committed store has completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+__device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
 // Generic-proxy shared-memory writes become visible to the tensor cores.

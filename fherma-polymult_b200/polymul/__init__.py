@@ -29,7 +29,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(os.path.dirname(HERE), "lib", "libfpm.so")
 
-FPM_OK, FPM_EINVAL, FPM_ECUDA, FPM_ENOMEM, FPM_EINTERNAL = 0, 1, 2, 3, 4
+FPM_OK, FPM_EINVAL, FPM_ECUDA, FPM_ENOMEM, FPM_EINTERNAL, FPM_ETIMEOUT = 0, 1, 2, 3, 4, 5
+STALL_DECOMPOSE, STALL_CRT = 1, 2
 MODE_PRODUCT, MODE_FORWARD = 0, 1
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
@@ -81,6 +82,11 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
                               ctypes.POINTER(FpmInfo), _u32p], ctypes.c_int),
         "fpm_run": ([vp, vp, vp, vp], ctypes.c_int),
         "fpm_run_device": ([vp, vp, vp, vp, vp], ctypes.c_int),
+        "fpm_run_device_noalloc": ([vp, vp, vp, vp, vp], ctypes.c_int),
+        "fpm_get_error": ([vp, vp], ctypes.c_int),
+        "fpm_noalloc_get_error": ([vp], ctypes.c_int),
+        "fpm_set_wait_limit": ([vp, ctypes.c_uint64], ctypes.c_int),
+        "fpm_debug_inject_stall": ([vp, ctypes.c_uint32], ctypes.c_int),
         "fpm_free": ([vp], None),
         "fpm_last_error": ([], ctypes.c_char_p),
         "fpm_get_info": ([vp, ctypes.POINTER(FpmInfo)], ctypes.c_int),
@@ -196,6 +202,20 @@ class Context:
     def run_device(self, d_a: int, d_b: int, d_c: int, stream: int = 0):
         """c = a b on device pointers (ints), enqueued on a cudaStream_t (int)."""
         _check(self._lib.fpm_run_device(self._h, d_a, d_b, d_c, stream or None))
+
+    def get_error(self, stream: int = 0) -> int:
+        """Waits for `stream`, then reads and clears the context's error word:
+        FPM_ETIMEOUT if a kernel pipeline wait ran out since the last check."""
+        return self._lib.fpm_get_error(self._h, stream or None)
+
+    def set_wait_limit(self, ns: int):
+        """Limit of every pipeline wait of later products, in nanoseconds."""
+        _check(self._lib.fpm_set_wait_limit(self._h, int(ns)))
+
+    def inject_stall(self, mask: int):
+        """Test hook: STALL_DECOMPOSE / STALL_CRT make that pipeline's wait run
+        out in later products (0 restores normal operation)."""
+        _check(self._lib.fpm_debug_inject_stall(self._h, mask))
 
     def stage_decompose(self, d_limbs: int, d_res: int, operand: int, stream: int = 0):
         _check(self._lib.fpm_stage_decompose(self._h, d_limbs, d_res, operand, stream or None))

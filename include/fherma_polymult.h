@@ -38,6 +38,7 @@ extern "C" {
 #define FPM_ECUDA 2     /* CUDA runtime failure */
 #define FPM_ENOMEM 3    /* device or host allocation failed */
 #define FPM_EINTERNAL 4 /* anything else */
+#define FPM_ETIMEOUT 5  /* a kernel pipeline wait ran out of time: the product's result is not valid */
 
 typedef struct fpm_ctx fpm_ctx;
 
@@ -86,9 +87,40 @@ FPM_API int fpm_run_device(fpm_ctx* ctx, const uint32_t* d_a, const uint32_t* d_
  * sizes.  The first call on each device looks up the array's address and
  * loads its module: make it before any stream capture.  All calls, from every
  * context, share the one array: calls whose work overlaps on the GPU race, so
- * order them on one stream. */
+ * order them on one stream.  The kernels are those of fpm_run_device.  A
+ * kernel whose pipeline wait runs out sets the array's error word, which
+ * stays set until fpm_noalloc_get_error reads and clears it. */
 FPM_API int fpm_run_device_noalloc(fpm_ctx* ctx, const uint32_t* d_a, const uint32_t* d_b, uint32_t* d_c,
                                    void* stream);
+
+/* Device-path errors (the reference reports CUDA failures by exception from
+ * fherma_run, solve.cu:84-88; the device entry points here return after
+ * enqueueing, so a failure inside their kernels is read afterwards).  Every
+ * wait inside the tensor-core kernels is bounded (2 s by default); one that
+ * runs out makes the kernel set a bit in an error word and return early, so
+ * the GPU never hangs but that product's c is wrong.  fpm_run checks the word
+ * itself and returns FPM_ETIMEOUT.
+ *
+ * fpm_get_error waits for the work enqueued on `stream`, then reads and
+ * clears the context's error word: FPM_ETIMEOUT if any product of this
+ * context since the last check (fpm_run_device, stage entry points) had a wait
+ * run out, FPM_OK otherwise.  fpm_noalloc_get_error does the same for the
+ * error word of the static scratch array on the current device, which every
+ * fpm_run_device_noalloc call on that device shares; it allocates nothing. */
+FPM_API int fpm_get_error(fpm_ctx* ctx, void* stream);
+FPM_API int fpm_noalloc_get_error(void* stream);
+
+/* The limit of every pipeline wait in the context's kernels, in nanoseconds
+ * (default 2e9); applies to products enqueued afterwards on this context
+ * (batches and servers copy it when they are created). */
+FPM_API int fpm_set_wait_limit(fpm_ctx* ctx, uint64_t ns);
+
+/* Test hook, for checking the error path without faulting the GPU: with mask
+ * bit 0 (decompose) or bit 1 (CRT) set, the pipelined kernel of later
+ * products on this context never requests one of its shared-memory copies, so
+ * the wait for it runs out after the wait limit and the call reports
+ * FPM_ETIMEOUT.  0 restores normal operation. */
+FPM_API int fpm_debug_inject_stall(fpm_ctx* ctx, uint32_t mask);
 
 /* Replaces fherma_free (reference fherma.h:48, solve.cu:1061-1083); accepts
  * NULL. */

@@ -177,13 +177,17 @@ def _ref_lib():
                                  _u32p, _u32p, _u32p]
         lib.ref_plan.restype = ctypes.c_int
         lib.ref_last_error.restype = ctypes.c_char_p
+        lib.ref_set_threads.argtypes = [ctypes.c_int]
+        lib.ref_set_threads.restype = ctypes.c_int
         _rlib = lib
     return _rlib
 
 
-def ref_polymul(N: int, W: int, q, a, b, reps: int = 1):
-    """The reference's fherma_run on (a, b): returns (c, seconds per call)."""
+def ref_polymul(N: int, W: int, q, a, b, reps: int = 1, threads: int = 0):
+    """The reference's fherma_run on (a, b): returns (c, seconds per call).
+    threads: OpenMP threads of the reference's loops (0: all processors)."""
     lib = _ref_lib()
+    lib.ref_set_threads(threads)
     q = np.ascontiguousarray(q, dtype=np.uint32)
     L = q.shape[0]
     a = np.ascontiguousarray(a, dtype=np.uint32)

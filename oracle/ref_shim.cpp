@@ -12,6 +12,8 @@
 #include "fherma.h"
 #include "rns_plan.h"
 
+#include <omp.h>
+
 #include <chrono>
 #include <cstring>
 #include <exception>
@@ -60,6 +62,13 @@ int ref_polymul(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, const uin
         if (state) fherma_free(state);
         return 1;
     }
+}
+
+// OpenMP threads for the reference's parallel loops (n <= 0: all processors).
+// Returns the count in effect.
+int ref_set_threads(int n) {
+    omp_set_num_threads(n > 0 ? n : omp_get_num_procs());
+    return n > 0 ? n : omp_get_num_procs();
 }
 
 // The reference's setup tables for (N, q[L]) (rns_plan.h:118-249), so the

@@ -7,7 +7,9 @@ in one static 80 MiB device array, so the call allocates nothing.  These tests
 call it through the C ABI and check it bit-exact (the tolerance of every
 integer test here) against fpm_run_device on the same operands, on two calls
 in a row, so the second call also shows that what the first left in the shared
-array does not leak into its result.  The file is named to be collected last:
+array does not leak into its result, and that the array's error word stays
+clear.  The cases cover the tensor-core pipelines (two or more limbs) and the
+one-limb CRT on the CUDA cores.  The file is named to be collected last:
 it passes alone in a fresh process, where its first call is the one that looks
 up the array's address, and after every other test.
 """
@@ -33,7 +35,8 @@ def noalloc_fn():
     return lib, fn
 
 
-@pytest.mark.parametrize("N,W,pattern", [(4096, 256, "uniform"), (65536, 2048, "max"), (2048, 1747, "uniform")])
+@pytest.mark.parametrize("N,W,pattern", [(4096, 256, "uniform"), (65536, 2048, "max"), (2048, 1747, "uniform"),
+                                         (4096, 32, "uniform")])
 def test_noalloc_matches_run_device_twice(cuda, N, W, pattern):
     torch = cuda
     lib, run_noalloc = noalloc_fn()
@@ -58,6 +61,7 @@ def test_noalloc_matches_run_device_twice(cuda, N, W, pattern):
             rc = run_noalloc(ctx.handle, da.data_ptr(), db.data_ptr(), dc.data_ptr(), stream)
             assert rc == polymul.FPM_OK, lib.fpm_last_error().decode()
             got.append(dc)
+        assert lib.fpm_noalloc_get_error(stream) == polymul.FPM_OK
         torch.cuda.synchronize()
         for e, g in zip(expect, got):
             assert torch.equal(e, g)
