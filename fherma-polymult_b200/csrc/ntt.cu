@@ -27,7 +27,9 @@
 #include "ntt_engine.cuh"
 #include "pdl.cuh"
 #include "tc.cuh"
+#include "tmap.h"
 
+#include <algorithm>
 #include <type_traits>
 
 namespace fpm {
@@ -203,6 +205,169 @@ __device__ __forceinline__ void col_inv_body(const DevPoint& d, uint32_t* A, int
         }
         col_global_store<LOGR, LOGS, RB, 0, 1>(X, v, base, c0);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Column passes staged through TMA (R = 64 rows: N = 2^12 .. 2^17).  With
+// 8-element rounds the column tile's shared layout (SwzCol) is exactly the
+// 128-byte TMA swizzle of a box of 64 rows x 32 words, so a tile arrives by
+// one cp.async.bulk.tensor load per operand and leaves by one tensor store;
+// the first and last rounds read and write shared memory.  The kernels are
+// persistent: a CTA walks tiles t = blockIdx.x + i gridDim.x (tile t = prime
+// t / per, column block t % per) through two buffers, the next tile's boxes and
+// its prime's 64 twiddles (a bulk copy) landing while the current tile is
+// transformed.  Tensor maps cover this GPU's own residue arrays only.
+
+constexpr uint32_t kColTmaBox = 2048 * sizeof(uint32_t);                 // one operand's tile
+constexpr uint32_t kColTmaTw = 64 * sizeof(uint2);                       // R = 64 twiddles
+constexpr uint32_t kColFwdStage = 17 * 1024;                             // A, B, twiddles (1024-aligned)
+constexpr uint32_t kColInvStage = 9 * 1024;                              // A, twiddles
+constexpr size_t kColFwdTmaSmem = 2 * size_t(kColFwdStage) + 16;
+constexpr size_t kColInvTmaSmem = 2 * size_t(kColInvStage) + 16;
+
+template <int LOGS, bool FWD>
+__device__ __forceinline__ void col_tma_issue(const DevPoint& d, const CUtensorMap* tmA, const CUtensorMap* tmB,
+                                              uint8_t* stage, uint64_t* bar, uint32_t t) {
+    constexpr uint32_t per = (1u << LOGS) / 32;
+    const uint32_t j = t / per, bx = t - (t / per) * per;
+    tc::mbar_arrive_expect_tx(bar, (FWD ? 2 : 1) * kColTmaBox + kColTmaTw);
+    tc::tma_load_2d(stage, tmA, static_cast<int>(bx * 32), static_cast<int>(j * 64), bar);
+    if constexpr (FWD) tc::tma_load_2d(stage + kColTmaBox, tmB, static_cast<int>(bx * 32), static_cast<int>(j * 64), bar);
+    const uint2* tw = (FWD ? d.col_f : d.col_i) + static_cast<size_t>(j) * 64;
+    tc::bulk_g2s(stage + (FWD ? 2 : 1) * kColTmaBox, tw, kColTmaTw, bar);
+}
+
+template <int LOGS, bool LAZY>
+__global__ void __launch_bounds__(256, 6)
+    k_ntt_col_fwd_tma(DevPoint d, const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    constexpr int LOGR = 6, XS = 5, RB = 3, E = 8;
+    using SWZ = SwzCol;
+    static_assert(RP<LOGR, XS, SWZ, RB>::all_conflict_free(), "column rounds must be free of bank conflicts");
+    constexpr int last = RP<LOGR, XS, SWZ, RB>::kCount - 1;
+    constexpr uint32_t per = (1u << LOGS) / 32;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + 2 * kColFwdStage);
+    const uint32_t tiles = per * static_cast<uint32_t>(d.K);
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&full[0], 1);
+        tc::mbar_init(&full[1], 1);
+        tc::fence_mbar_init();
+        tc::prefetch_tmap(&tmA);
+        tc::prefetch_tmap(&tmB);
+    }
+    __syncthreads();
+    pdl_launch_dependents();
+    pdl_wait();
+    if (threadIdx.x == 0 && blockIdx.x < tiles) col_tma_issue<LOGS, true>(d, &tmA, &tmB, smem_raw, &full[0], blockIdx.x);
+    uint32_t i = 0;
+    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++i) {
+        const int s = i & 1;
+        uint8_t* stage = smem_raw + s * kColFwdStage;
+        uint32_t* const tiles2[2] = {reinterpret_cast<uint32_t*>(stage), reinterpret_cast<uint32_t*>(stage + kColTmaBox)};
+        const SharedTable table{reinterpret_cast<const uint2*>(stage + 2 * kColTmaBox)};
+        const uint32_t j = t / per;
+        const uint32_t p = d.pc[j].p;
+        if (!tc::wait_parity(&full[s], (i >> 1) & 1, d.wait_ns) && threadIdx.x == 0) atomicOr(d.err, 4u);
+        {
+            const uint32_t base = round_base<LOGR, XS, SWZ, RB, 0>(threadIdx.x);
+            uint32_t v[2][E];
+#pragma unroll
+            for (int o = 0; o < 2; ++o) load_round<LOGR, XS, SWZ, RB, 0>(tiles2[o], v[o], base);
+            fwd_round<LOGR, XS, SWZ, RB, 0, LAZY, 2>(v, base, table, p);
+#pragma unroll
+            for (int o = 0; o < 2; ++o) store_round<LOGR, XS, SWZ, RB, 0>(tiles2[o], v[o], base);
+            __syncthreads();
+        }
+        // The next tile's loads, into the other buffer once the stores of the
+        // tile that used it have read it.
+        if (threadIdx.x == 0 && t + gridDim.x < tiles) {
+            tc::bulk_wait_read();
+            col_tma_issue<LOGS, true>(d, &tmA, &tmB, smem_raw + (s ^ 1) * kColFwdStage, &full[s ^ 1], t + gridDim.x);
+        }
+        fwd_range<LOGR, XS, SWZ, RB, 1, last, LAZY, 2>(tiles2, table, p);
+        {
+            const uint32_t base = round_base<LOGR, XS, SWZ, RB, last>(threadIdx.x);
+            uint32_t v[2][E];
+#pragma unroll
+            for (int o = 0; o < 2; ++o) load_round<LOGR, XS, SWZ, RB, last>(tiles2[o], v[o], base);
+            fwd_round<LOGR, XS, SWZ, RB, last, LAZY, 2>(v, base, table, p);
+#pragma unroll
+            for (int o = 0; o < 2; ++o) store_round<LOGR, XS, SWZ, RB, last>(tiles2[o], v[o], base);
+        }
+        tc::fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const uint32_t bx = t - j * per;
+            tc::tma_store_2d(&tmA, tiles2[0], static_cast<int>(bx * 32), static_cast<int>(j * 64));
+            tc::tma_store_2d(&tmB, tiles2[1], static_cast<int>(bx * 32), static_cast<int>(j * 64));
+            tc::bulk_commit();
+        }
+    }
+    if (threadIdx.x == 0) tc::bulk_wait_all();
+}
+
+template <int LOGS, bool LAZY>
+__global__ void __launch_bounds__(256, 8) k_ntt_col_inv_tma(DevPoint d, const __grid_constant__ CUtensorMap tmA) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    constexpr int LOGR = 6, XS = 5, RB = 3, E = 8;
+    using SWZ = SwzCol;
+    static_assert(RP<LOGR, XS, SWZ, RB>::all_conflict_free(), "column rounds must be free of bank conflicts");
+    constexpr int last = RP<LOGR, XS, SWZ, RB>::kCount - 1;
+    constexpr uint32_t per = (1u << LOGS) / 32;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + 2 * kColInvStage);
+    const uint32_t tiles = per * static_cast<uint32_t>(d.K);
+    if (threadIdx.x == 0) {
+        tc::mbar_init(&full[0], 1);
+        tc::mbar_init(&full[1], 1);
+        tc::fence_mbar_init();
+        tc::prefetch_tmap(&tmA);
+    }
+    __syncthreads();
+    pdl_launch_dependents();
+    pdl_wait();
+    if (threadIdx.x == 0 && blockIdx.x < tiles) col_tma_issue<LOGS, false>(d, &tmA, &tmA, smem_raw, &full[0], blockIdx.x);
+    uint32_t i = 0;
+    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++i) {
+        const int s = i & 1;
+        uint8_t* stage = smem_raw + s * kColInvStage;
+        uint32_t* ta = reinterpret_cast<uint32_t*>(stage);
+        const SharedTable table{reinterpret_cast<const uint2*>(stage + kColTmaBox)};
+        const uint32_t j = t / per;
+        const uint32_t p = d.pc[j].p;
+        if (!tc::wait_parity(&full[s], (i >> 1) & 1, d.wait_ns) && threadIdx.x == 0) atomicOr(d.err, 4u);
+        {
+            const uint32_t base = round_base<LOGR, XS, SWZ, RB, last>(threadIdx.x);
+            uint32_t v[E];
+            load_round<LOGR, XS, SWZ, RB, last>(ta, v, base);
+            inv_round<LOGR, XS, SWZ, RB, last, LAZY, false>(v, base, table, p);
+            store_round<LOGR, XS, SWZ, RB, last>(ta, v, base);
+            __syncthreads();
+        }
+        if (threadIdx.x == 0 && t + gridDim.x < tiles) {
+            tc::bulk_wait_read();
+            col_tma_issue<LOGS, false>(d, &tmA, &tmA, smem_raw + (s ^ 1) * kColInvStage, &full[s ^ 1], t + gridDim.x);
+        }
+        inv_range<LOGR, XS, SWZ, RB, last - 1, 1, LAZY, false>(ta, table, p);
+        {
+            const uint32_t base = round_base<LOGR, XS, SWZ, RB, 0>(threadIdx.x);
+            uint32_t v[E];
+            load_round<LOGR, XS, SWZ, RB, 0>(ta, v, base);
+            inv_round<LOGR, XS, SWZ, RB, 0, LAZY, false>(v, base, table, p);
+            if constexpr (LAZY) {
+#pragma unroll
+                for (int k = 0; k < E; ++k) v[k] = reduce_once(v[k], p);   // y_j canonical for the CRT
+            }
+            store_round<LOGR, XS, SWZ, RB, 0>(ta, v, base);
+        }
+        tc::fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const uint32_t bx = t - j * per;
+            tc::tma_store_2d(&tmA, ta, static_cast<int>(bx * 32), static_cast<int>(j * 64));
+            tc::bulk_commit();
+        }
+    }
+    if (threadIdx.x == 0) tc::bulk_wait_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -651,8 +816,24 @@ void group_pass(const GroupTable* t, int pass, uint32_t logR, uint32_t logS, uin
     }
 }
 
+template <int LOGS, bool LAZY>
+void col_tma_attrs() {
+    check(cudaFuncSetAttribute(k_ntt_col_fwd_tma<LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(kColFwdTmaSmem)),
+          "col smem");
+    check(cudaFuncSetAttribute(k_ntt_col_inv_tma<LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(kColInvTmaSmem)),
+          "col smem");
+}
+
 template <bool LAZY>
 void attrs_all() {
+    col_tma_attrs<6, LAZY>();
+    col_tma_attrs<7, LAZY>();
+    col_tma_attrs<8, LAZY>();
+    col_tma_attrs<9, LAZY>();
+    col_tma_attrs<10, LAZY>();
+    col_tma_attrs<11, LAZY>();
     for (uint32_t s = 6; s <= 11; ++s)
         with_cols(6, s, [&](auto lr, auto ls) { col_attrs<decltype(lr)::value, decltype(ls)::value, LAZY>(); });
     for (uint32_t r = 7; r <= 11; ++r)
@@ -665,8 +846,41 @@ void attrs_all() {
     row_attrs<11, LAZY>();
 }
 
+// SMs of the current device (the persistent column grids take one slot per
+// resident CTA).
+int device_sms() {
+    static int cached[64] = {};
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (dev < 0 || dev >= 64) dev = 0;
+    if (!cached[dev]) check(cudaDeviceGetAttribute(&cached[dev], cudaDevAttrMultiProcessorCount, dev), "SM count");
+    return cached[dev];
+}
+
+// The TMA column passes take R = 64 and 16-byte aligned residue arrays.
+bool col_tma_ok(const DevPoint& d, const uint32_t* A, const uint32_t* B) {
+    return d.logR == 6 && d.logS >= 6 && d.logS <= 11 && (reinterpret_cast<uintptr_t>(A) & 15) == 0 &&
+           (reinterpret_cast<uintptr_t>(B) & 15) == 0;
+}
+
+// The residues K x N viewed as K R rows of S words.
+CUtensorMap col_tmap(const DevPoint& d, const uint32_t* X) {
+    return make_tmap_u32(X, static_cast<uint64_t>(d.K) << 6, d.N >> 6, d.N >> 6, 64, 32, TmaSwizzle::k128B);
+}
+
 template <bool LAZY>
 void launch_col_fwd_t(const DevPoint& d, uint32_t* A, uint32_t* B, cudaStream_t st) {
+    if (col_tma_ok(d, A, B)) {
+        with_log(d.logS, [&](auto s) {
+            constexpr int LS = decltype(s)::value;
+            const uint32_t tiles = ((1u << LS) / 32) * static_cast<uint32_t>(d.K);
+            const uint32_t grid = std::min<uint32_t>(tiles, 6u * static_cast<uint32_t>(device_sms()));
+            check(launch_pdl(k_ntt_col_fwd_tma<LS, LAZY>, dim3(grid), dim3(256), kColFwdTmaSmem, st, d, col_tmap(d, A),
+                             col_tmap(d, B)),
+                  "col_fwd launch");
+        });
+        return;
+    }
     with_cols(d.logR, d.logS, [&](auto r, auto s) {
         constexpr int LR = decltype(r)::value, LS = decltype(s)::value;
         const dim3 grid(col_blocks<LR>(LS), d.K);
@@ -678,6 +892,17 @@ void launch_col_fwd_t(const DevPoint& d, uint32_t* A, uint32_t* B, cudaStream_t 
 
 template <bool LAZY>
 void launch_col_inv_t(const DevPoint& d, uint32_t* A, cudaStream_t st) {
+    if (col_tma_ok(d, A, A)) {
+        with_log(d.logS, [&](auto s) {
+            constexpr int LS = decltype(s)::value;
+            const uint32_t tiles = ((1u << LS) / 32) * static_cast<uint32_t>(d.K);
+            const uint32_t grid = std::min<uint32_t>(tiles, 8u * static_cast<uint32_t>(device_sms()));
+            check(launch_pdl(k_ntt_col_inv_tma<LS, LAZY>, dim3(grid), dim3(256), kColInvTmaSmem, st, d,
+                             col_tmap(d, A)),
+                  "col_inv launch");
+        });
+        return;
+    }
     with_cols(d.logR, d.logS, [&](auto r, auto s) {
         constexpr int LR = decltype(r)::value, LS = decltype(s)::value;
         const dim3 grid(col_blocks<LR>(LS), d.K);
