@@ -609,6 +609,7 @@ def main():
             ctx.run(a_, b_, c_)
         return (time.perf_counter() - t0) * 1e6 / n
 
+    io_chunks = ctx.tune_host_path()   # as fherma_init does, outside the timed calls
     e2e_us = e2e(a_p, b_p, c_p, args.e2e_steps)
     c_h = np.empty((N, L), np.uint32)
     e2e_pageable_us = e2e(a_h, b_h, c_h, args.e2e_steps)
@@ -660,6 +661,31 @@ def main():
 
     sustained = measure_sustained(torch, ctx, sets_d, stream) if rank == 0 else None
 
+    # Context set-up (fpm_init): a new modulus of the width in use (the prime
+    # basis's tables are shared, the CRT tables are built on the device), a
+    # width not yet in use (the whole basis built and uploaded), and the
+    # host-only plan of the same point for comparison.
+    init = None
+    if rank == 0:
+        rng_i = np.random.Generator(np.random.PCG64(6000))
+
+        def init_us(width):
+            qq = workload.random_modulus(width, rng_i)
+            t0 = time.perf_counter()
+            c_ = polymul.Context(N, width, qq)
+            t1 = time.perf_counter()
+            c_.close()
+            return (t1 - t0) * 1e6
+
+        warm = sorted(init_us(W) for _ in range(5))
+        cold = init_us(W - 1)
+        t0 = time.perf_counter()
+        polymul.plan_info(N, W, workload.random_modulus(W, rng_i))
+        host_plan = (time.perf_counter() - t0) * 1e6
+        init = {"new_modulus_us": statistics.median(warm), "new_width_us": cold, "host_plan_us": host_plan,
+                "note": f"fpm_init at N={N}: a new W={W} modulus while a context of that width is open (median of "
+                        f"5), a W={W - 1} modulus (a basis not yet built), and make_plan alone on the host"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -710,7 +736,8 @@ def main():
                        "l2": f"{ROTATE} operand sets rotate ({ROTATE * 3 * N * L * 4 / 1e6:.0f} MB > 126 MB L2)"},
             "products_per_s": 1e6 / us_per_product,
             "e2e": {"value": e2e_us, "unit": "us/product", "h2d_bytes_per_step": 2 * N * L * 4,
-                    "d2h_bytes_per_step": N * L * 4, "host_buffers": "pinned (fpm_run, wall clock)"},
+                    "d2h_bytes_per_step": N * L * 4, "host_buffers": "pinned (fpm_run, wall clock)",
+                    "io_chunks": io_chunks, "calls": args.e2e_steps},
             "e2e_pageable": {"value": e2e_pageable_us, "unit": "us/product",
                              "host_buffers": "pageable numpy (fpm_run stages through pinned memory)"},
             "pcie": link,
@@ -729,6 +756,7 @@ def main():
             "gpu_launches": args.steps * launches_per_product,
             "clocks": clocks,
             "sustained": sustained,
+            "init": init,
             "configs": points,
             "cpu_baseline": cpu,
             "batched": batched,

@@ -69,7 +69,7 @@ int resolve_prime_bits(int prime_bits) {
     return fpm::kDefaultPrimeBits;
 }
 
-void fill_info(const fpm::HostPlan& pl, uint32_t W, int device, fpm_info* out) {
+void fill_info(const fpm::HostPlan& pl, uint32_t W, int device, size_t device_bytes, fpm_info* out) {
     out->N = pl.N;
     out->W = W;
     out->L = static_cast<uint32_t>(pl.L);
@@ -78,7 +78,7 @@ void fill_info(const fpm::HostPlan& pl, uint32_t W, int device, fpm_info* out) {
     out->logR = pl.g.logR;
     out->logS = pl.g.logS;
     out->device = device;
-    out->device_bytes = fpm::device_footprint(pl);
+    out->device_bytes = device_bytes;
     out->prime_bits = static_cast<uint32_t>(pl.pmax_log2);
 }
 
@@ -175,7 +175,7 @@ void fpm_free(fpm_ctx* ctx) {
 
 int fpm_get_info(const fpm_ctx* ctx, fpm_info* out) {
     if (!ctx || !out) return fail(FPM_EINVAL, "fpm_get_info: NULL argument");
-    fill_info(ctx->engine->plan(), ctx->W, ctx->engine->device(), out);
+    fill_info(ctx->engine->plan(), ctx->W, ctx->engine->device(), ctx->engine->device_bytes(), out);
     return FPM_OK;
 }
 
@@ -190,7 +190,7 @@ int fpm_plan_info_ex(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, int 
     if (bits != 30 && bits != 31) return fail(FPM_EINVAL, "prime_bits must be 30 or 31");
     return guarded([&] {
         const fpm::HostPlan pl = fpm::make_plan(N, W, q, static_cast<int>(L), bits);
-        fill_info(pl, W, -1, out);
+        fill_info(pl, W, -1, fpm::device_footprint(pl), out);
         if (primes) {
             for (int j = 0; j < pl.K; ++j) primes[j] = pl.primes[j];
         }
@@ -202,6 +202,19 @@ int fpm_get_primes(const fpm_ctx* ctx, uint32_t* out) {
     const auto& p = ctx->engine->plan().primes;
     for (size_t i = 0; i < p.size(); ++i) out[i] = p[i];
     return FPM_OK;
+}
+
+int fpm_tune_host_path(fpm_ctx* ctx, int* chunks) {
+    if (!ctx) return fail(FPM_EINVAL, "fpm_tune_host_path: NULL context");
+    return guarded([&] {
+        const int n = ctx->engine->tune_host_path();
+        if (chunks) *chunks = n;
+    });
+}
+
+int fpm_get_crt_tables(const fpm_ctx* ctx, uint32_t* M, uint32_t* negvP) {
+    if (!ctx || !M || !negvP) return fail(FPM_EINVAL, "fpm_get_crt_tables: NULL argument");
+    return guarded([&] { ctx->engine->crt_tables(M, negvP); });
 }
 
 int fpm_stage_decompose(fpm_ctx* ctx, const uint32_t* d_limbs, uint32_t* d_res, int operand, void* stream) {
@@ -317,6 +330,11 @@ int fpm_server_create(fpm_ctx* const* points, uint32_t count, uint64_t budget_by
     return FPM_OK;
 }
 
+int fpm_server_add_point(fpm_server* srv, fpm_ctx* point, uint32_t* index) {
+    if (!srv || !point || !index) return fail(FPM_EINVAL, "fpm_server_add_point: NULL argument");
+    return guarded([&] { *index = srv->server->add_point(point->engine); });
+}
+
 int fpm_server_footprint(const fpm_server* srv, uint32_t point, uint64_t* bytes) {
     if (!srv || !bytes) return fail(FPM_EINVAL, "fpm_server_footprint: NULL argument");
     return guarded([&] { *bytes = srv->server->footprint(point); });
@@ -374,6 +392,13 @@ void* fherma_init(const fherma::Point& p) {
     }
     fpm_ctx* ctx = nullptr;
     if (fpm_init(p.N, p.W, p.L, p.q.data.data(), &ctx) != FPM_OK) throw std::runtime_error(fpm_last_error());
+    // As the reference's init measures its copy modes, set-up measures the
+    // host path's chunking here, outside the timed fherma_run calls.
+    if (fpm_tune_host_path(ctx, nullptr) != FPM_OK) {
+        const std::string msg = fpm_last_error();
+        fpm_free(ctx);
+        throw std::runtime_error(msg);
+    }
     return ctx;
 }
 

@@ -507,16 +507,13 @@ void set_attr() {
 
 }  // namespace
 
-CrtConsts make_crt_consts(const HostPlan& pl) {
+CrtConsts make_crt_consts(const HostPlan& pl, const uint32_t* top) {
     CrtConsts cc{};
-    for (int j = 0; j < pl.K; ++j) {
-        cc.r50[j] = static_cast<uint32_t>((1ull << 50) / pl.primes[j]);
-        const uint32_t top = pl.M[static_cast<size_t>(j) * pl.L + pl.L - 1];
-        cc.mlo[j] = top & 0xFFFFu;
-        cc.mhi[j] = top >> 16;
+    for (int j = 0; j <= pl.K; ++j) {
+        if (j < pl.K) cc.r50[j] = static_cast<uint32_t>((1ull << 50) / pl.primes[j]);
+        cc.mlo[j] = top[j] & 0xFFFFu;
+        cc.mhi[j] = top[j] >> 16;
     }
-    cc.mlo[pl.K] = pl.negp_top & 0xFFFFu;
-    cc.mhi[pl.K] = pl.negp_top >> 16;
     for (int k = 0; k < pl.L; ++k) cc.q[k] = pl.q[k];
     return cc;
 }

@@ -9,10 +9,13 @@
 #include "kernels.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <stdexcept>
+#include <tuple>
 
 namespace fpm {
 
@@ -33,11 +36,122 @@ void ensure_kernel_attributes(int device) {
     done.push_back(device);
 }
 
+namespace {
+
+// Device allocations of a shared prime basis.
+struct DeviceBlocks {
+    std::vector<void*> ptrs;
+    size_t bytes = 0;
+    template <class T>
+    T* alloc(size_t count) {
+        void* p = nullptr;
+        const size_t b = std::max<size_t>(count, 1) * sizeof(T);
+        check(cudaMalloc(&p, b), "cudaMalloc");
+        ptrs.push_back(p);
+        bytes += b;
+        return static_cast<T*>(p);
+    }
+    template <class T>
+    const T* upload(const std::vector<T>& v) {
+        if (v.empty()) return nullptr;
+        T* d = alloc<T>(v.size());
+        check(cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
+        return d;
+    }
+    void release() {
+        for (void* p : ptrs) cudaFree(p);
+        ptrs.clear();
+        bytes = 0;
+    }
+};
+
+template <class T>
+void drop(std::vector<T>& v) {
+    std::vector<T>().swap(v);
+}
+
+}  // namespace
+
+// The tables of one prime basis on one device: everything a point's kernels
+// read that depends on q only through its bit length (make_plan_basis), among
+// them the row pass's K x N twiddle tables.  Every Engine on the device whose
+// (N, L, bits of q, prime window) match shares one Basis, so a context for a
+// new modulus of a width already in use uploads nothing but q and builds its
+// CRT tables on the device.
+struct Engine::Basis {
+    HostPlan plan;            // no modulus; the big host tables are dropped after upload
+    DevPoint dp{};            // the basis tables' device pointers
+    DeviceBlocks mem;
+    std::shared_ptr<const DecConsts> dec;
+    ~Basis() { mem.release(); }
+
+    static std::shared_ptr<Basis> get(int device, uint32_t N, uint32_t W, int L, int qbits, int pmax_log2) {
+        static std::mutex mu;
+        static std::map<std::tuple<int, uint32_t, int, int, int>, std::weak_ptr<Basis>> cache;
+        const auto key = std::make_tuple(device, N, L, qbits, pmax_log2);
+        std::lock_guard<std::mutex> lock(mu);
+        if (auto b = cache[key].lock()) return b;
+        std::shared_ptr<Basis> b(new Basis());
+        b->build(make_plan_basis(N, W, L, qbits, pmax_log2));
+        cache[key] = b;
+        return b;
+    }
+
+private:
+    void build(HostPlan pl) {
+        DevPoint& d = dp;
+        d.N = pl.N;
+        d.logN = pl.g.logN;
+        d.logR = pl.g.logR;
+        d.logS = pl.g.logS;
+        d.L = pl.L;
+        d.K = pl.K;
+        d.lazy = pl.lazy ? 1 : 0;
+        d.pc = mem.upload(pl.pc);
+        d.dec_a = mem.upload(pl.dec_a);
+        d.dec_b = mem.upload(pl.dec_b);
+        d.col_f = mem.upload(pl.col_f);
+        d.col_i = mem.upload(pl.col_i);
+        d.row_u_f = mem.upload(pl.row_u_f);
+        d.row_q_f = mem.upload(pl.row_q_f);
+        d.row_tw = nullptr;
+        d.full_f = mem.upload(pl.full_f);
+        d.full_i = mem.upload(pl.full_i);
+        d.p_recip = mem.upload(pl.p_recip);
+        d.dec_kb = pl.dec_kb;
+        d.dec_chunks = static_cast<int>(pl.dec_chunks);
+        d.dec_img_a = mem.upload(pl.dec_img_a);
+        d.dec_img_b = mem.upload(pl.dec_img_b);
+        d.dec_fold = mem.upload(pl.dec_fold);
+        d.crt_u = pl.crt_u;
+        d.crt_tmem_cols = pl.crt_tmem_cols;
+        d.wait_ns = kDefaultWaitNs;
+        d.fault = 0;
+        if (decompose_pipe_supported(pl)) {
+            const uint8_t* wa = mem.upload(pl.dec_wimg_a);
+            const uint8_t* wb = mem.upload(pl.dec_wimg_b);
+            dec.reset(new DecConsts(make_dec_consts(pl, wa, wb)));
+        }
+        if (!pl.g.small) {
+            uint2* tw = mem.alloc<uint2>(static_cast<size_t>(pl.K) * pl.N);
+            build_row_tables(d, tw, nullptr);
+            check(cudaDeviceSynchronize(), "row tables");
+            d.row_tw = tw;
+        }
+        for (auto* v : {&pl.dec_a, &pl.dec_b, &pl.col_f, &pl.col_i, &pl.row_u_f, &pl.row_q_f, &pl.full_f, &pl.full_i})
+            drop(*v);
+        for (auto* v : {&pl.dec_img_a, &pl.dec_img_b, &pl.dec_wimg_a, &pl.dec_wimg_b}) drop(*v);
+        plan = std::move(pl);
+    }
+};
+
 template <class T>
 T* Engine::dalloc(size_t count) {
     void* p = nullptr;
-    check(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)), "cudaMalloc");
+    const size_t b = std::max<size_t>(count, 1) * sizeof(T);
+    check(cudaMalloc(&p, b), "cudaMalloc");
     dmem_.push_back(p);
+    own_bytes_ += b;
     return static_cast<T*>(p);
 }
 
@@ -49,59 +163,53 @@ const T* Engine::upload(const std::vector<T>& v) {
     return d;
 }
 
-Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
-    : plan_(make_plan(N, W, q, L, pmax_log2)) {
+Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2) {
     try {
         check(cudaGetDevice(&device_), "cudaGetDevice");
         check(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_), "SM count");
         ensure_kernel_attributes(device_);
+        // The point is checked before any device work (N first, as make_plan does).
+        check_length(N);
+        const int qbits = modulus_bits(q, L);
+        basis_ = Basis::get(device_, N, W, L, qbits, pmax_log2);
+        plan_ = basis_->plan;
+        plan_.W = W;
+        set_modulus_limbs(plan_, q);
         const HostPlan& pl = plan_;
-        dp_.N = pl.N;
-        dp_.logN = pl.g.logN;
-        dp_.logR = pl.g.logR;
-        dp_.logS = pl.g.logS;
-        dp_.L = pl.L;
-        dp_.K = pl.K;
-        dp_.pc = upload(pl.pc);
-        dp_.dec_a = upload(pl.dec_a);
-        dp_.dec_b = upload(pl.dec_b);
-        dp_.col_f = upload(pl.col_f);
-        dp_.col_i = upload(pl.col_i);
-        dp_.row_u_f = upload(pl.row_u_f);
-        dp_.row_q_f = upload(pl.row_q_f);
-        dp_.row_tw = nullptr;
-        dp_.lazy = pl.lazy ? 1 : 0;
-        dp_.full_f = upload(pl.full_f);
-        dp_.full_i = upload(pl.full_i);
+        const int K = pl.K;
+        dp_ = basis_->dp;
+        dec_consts_ = basis_->dec;
         dp_.q = upload(pl.q);
         dp_.q_top = pl.q_top;
         dp_.q_top_inv = 1.0 / pl.q_top;
-        dp_.M = upload(pl.M);
-        dp_.negvP = upload(pl.negvP);
-        dp_.p_recip = upload(pl.p_recip);
-        dp_.dec_kb = pl.dec_kb;
-        dp_.dec_chunks = static_cast<int>(pl.dec_chunks);
-        dp_.dec_img_a = upload(pl.dec_img_a);
-        dp_.dec_img_b = upload(pl.dec_img_b);
-        dp_.dec_fold = upload(pl.dec_fold);
-        dp_.crt_u = pl.crt_u;
-        dp_.crt_tmem_cols = pl.crt_tmem_cols;
-        dp_.crt_img = upload(pl.crt_img);
-        dp_.crt_img_v = upload(pl.crt_img_v);
-        dp_.negp_top = pl.negp_top;
-        dp_.wait_ns = kDefaultWaitNs;
-        dp_.fault = 0;
-        if (crt_uses_tc(pl)) crt_consts_.reset(new CrtConsts(make_crt_consts(pl)));
-        if (decompose_pipe_supported(pl)) {
-            const uint8_t* wa = upload(pl.dec_wimg_a);
-            const uint8_t* wb = upload(pl.dec_wimg_b);
-            dec_consts_.reset(new DecConsts(make_dec_consts(pl, wa, wb)));
+        // The modulus tables, built on the device from the basis's primes.
+        uint32_t* M = dalloc<uint32_t>(static_cast<size_t>(K) * L);
+        uint32_t* negvP = dalloc<uint32_t>(static_cast<size_t>(K + 1) * L);
+        uint32_t* Pq = dalloc<uint32_t>(static_cast<size_t>(L));
+        uint8_t* img = nullptr;
+        uint8_t* img_v = nullptr;
+        if (crt_uses_tc(pl)) {
+            img = dalloc<uint8_t>(crt_image_bytes(pl, K));
+            img_v = dalloc<uint8_t>(crt_image_bytes(pl, K + 1));
         }
-        if (!pl.g.small) {
-            uint2* tw = dalloc<uint2>(static_cast<size_t>(pl.K) * pl.N);
-            build_row_tables(dp_, tw, nullptr);
-            check(cudaDeviceSynchronize(), "row tables");
-            dp_.row_tw = tw;
+        build_crt_tables(pl, dp_.pc, dp_.q, M, negvP, Pq, img, img_v, nullptr);
+        dp_.M = M;
+        dp_.negvP = negvP;
+        dp_.crt_img = img;
+        dp_.crt_img_v = img_v;
+        if (crt_uses_tc(pl)) {
+            // The CRT pipeline's parameters need the constants' top limbs.
+            std::vector<uint32_t> tops(static_cast<size_t>(K) + 1);
+            check(cudaMemcpy2D(tops.data(), sizeof(uint32_t), M + (L - 1), static_cast<size_t>(L) * 4,
+                               sizeof(uint32_t), static_cast<size_t>(K), cudaMemcpyDeviceToHost),
+                  "CRT top limbs");
+            check(cudaMemcpy(&tops[K], negvP + L + (L - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost),
+                  "CRT top limb");
+            plan_.negp_top = tops[K];
+            dp_.negp_top = tops[K];
+            crt_consts_.reset(new CrtConsts(make_crt_consts(plan_, tops.data())));
+        } else {
+            check(cudaDeviceSynchronize(), "CRT tables");
         }
         dp_.err = dalloc<uint32_t>(1);
         check(cudaMemset(dp_.err, 0, sizeof(uint32_t)), "memset");
@@ -115,6 +223,15 @@ Engine::Engine(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2)
         release();
         throw;
     }
+}
+
+size_t Engine::device_bytes() const { return own_bytes_ + (basis_ ? basis_->mem.bytes : 0); }
+
+uint32_t Engine::crt_tables(uint32_t* M, uint32_t* negvP) const {
+    const size_t K = static_cast<size_t>(plan_.K), L = static_cast<size_t>(plan_.L);
+    check(cudaMemcpy(M, dp_.M, K * L * 4, cudaMemcpyDeviceToHost), "read M");
+    check(cudaMemcpy(negvP, dp_.negvP, (K + 1) * L * 4, cudaMemcpyDeviceToHost), "read negvP");
+    return static_cast<uint32_t>(K);
 }
 
 Engine::~Engine() { release(); }
@@ -232,21 +349,63 @@ void Engine::ensure_host_path() {
     // I/O chunks: equal slices on 128-coefficient boundaries, so a chunk's
     // decompose and CRT blocks never straddle two.  Each chunk costs about
     // 13 us of launches and pipeline start-up, so the default aims at 16 MiB of
-    // operand limbs per chunk, 1 to 4 chunks (N = 65536 at 2048 bits: 2 chunks,
-    // 1092 us a product against 1113 with 4 and 1166 with 8).  FPM_IO_CHUNKS
-    // overrides it.
+    // operand limbs per chunk, 1 to 4 chunks; tune_host_path() measures the
+    // candidates on this point.  FPM_IO_CHUNKS overrides both.
     const size_t in_bytes = 2 * bytes;
     int want = static_cast<int>(std::min<size_t>(4, std::max<size_t>(1, (in_bytes + (size_t(8) << 20)) >> 24)));
     if (const char* v = std::getenv("FPM_IO_CHUNKS")) want = std::max(1, std::atoi(v));
+    set_chunks(want);
+    pool_.reset(new CopyPool(default_copy_threads()));
+}
+
+void Engine::set_chunks(int want) {
     const uint32_t N = plan_.N;
     const uint32_t unit = 128;
     const uint32_t units = (N + unit - 1) / unit;
-    const uint32_t nch = std::min<uint32_t>(static_cast<uint32_t>(want), units);
+    const uint32_t nch = std::min<uint32_t>(static_cast<uint32_t>(std::max(1, want)), units);
     chunk_at_.clear();
     for (uint32_t k = 0; k <= nch; ++k) chunk_at_.push_back(std::min(N, units * k / nch * unit));
-    events_.resize(4 * nch);
+    for (auto e : events_) cudaEventDestroy(e);
+    events_.assign(4 * nch, nullptr);
     for (auto& e : events_) check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
-    pool_.reset(new CopyPool(default_copy_threads()));
+}
+
+// The reference's fherma_init times its candidate copy modes on the point
+// (solve.cu:805-862) and keeps the default unless another is at least 5%
+// faster.  Here the mode follows from the caller's buffers (pinned: DMA from
+// them directly; pageable: staged through pinned memory), and what the point
+// decides is how many chunks the copies are cut into: 1 to 4 candidates, each
+// run 1 + 3 times on the engine's own pinned buffers, median kept.
+int Engine::tune_host_path() {
+    ensure_host_path();
+    if (std::getenv("FPM_IO_CHUNKS")) return static_cast<int>(chunk_at_.size() - 1);
+    const int dflt = static_cast<int>(chunk_at_.size() - 1);
+    const size_t bytes = words() * sizeof(uint32_t);
+    std::memset(ha_, 0, bytes);
+    std::memset(hb_, 0, bytes);
+    auto time_it = [&](int n) {
+        set_chunks(n);
+        run_host(ha_, hb_, hc_);
+        double t[3];
+        for (double& x : t) {
+            const auto t0 = std::chrono::steady_clock::now();
+            run_host(ha_, hb_, hc_);
+            x = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        }
+        std::sort(t, t + 3);
+        return t[1];
+    };
+    const double base = time_it(dflt);
+    int best = dflt;
+    double best_t = base;
+    for (int n = 1; n <= 4; ++n) {
+        if (n == dflt) continue;
+        const double t = time_it(n);
+        if (t < best_t) best_t = t, best = n;
+    }
+    if (best_t > 0.95 * base) best = dflt;
+    set_chunks(best);
+    return best;
 }
 
 void Engine::run_host(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* (*out_fn)(void*),

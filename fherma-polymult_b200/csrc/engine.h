@@ -57,6 +57,11 @@ public:
     void run_host(const uint32_t* a, const uint32_t* b, uint32_t* c, uint32_t* (*out_fn)(void*) = nullptr,
                   void* out_arg = nullptr);
 
+    // Measures the host path's chunk counts on this point and keeps the
+    // fastest (the default unless another is 5% faster); returns the count.
+    // Synchronous, about a dozen products' time; fherma_init calls it.
+    int tune_host_path();
+
     // Stages, for checks against the oracle.
     void decompose(const uint32_t* d_limbs, uint32_t* d_res, int operand, cudaStream_t st);
     void transform(uint32_t* d_A, uint32_t* d_B, int mode, cudaStream_t st);
@@ -78,6 +83,14 @@ public:
     // afterwards leave one barrier phase without its arrival.
     void set_fault(uint32_t mask) { dp_.fault = mask; }
 
+    // Device bytes this context uses: its own buffers plus its prime basis's
+    // tables, which contexts with the same (N, L, bits of q, prime window) on
+    // the device share.
+    size_t device_bytes() const;
+    // Copies the CRT tables built on the device, M (K x L) and negvP
+    // ((K + 1) x L), to host memory; returns K.
+    uint32_t crt_tables(uint32_t* M, uint32_t* negvP) const;
+
     size_t words() const { return static_cast<size_t>(plan_.N) * plan_.L; }
     size_t residues() const { return static_cast<size_t>(plan_.K) * plan_.N; }
 
@@ -93,13 +106,17 @@ private:
     void launch_crt_any(const DevPoint& d, const uint32_t* d_y, uint32_t* d_c, uint32_t n0, uint32_t n1,
                         cudaStream_t st);
     void ensure_host_path();
+    void set_chunks(int want);
     template <class T>
     T* dalloc(size_t count);
     template <class T>
     const T* upload(const std::vector<T>& v);
 
-    HostPlan plan_;
+    struct Basis;
+    std::shared_ptr<Basis> basis_;   // shared tables of the prime basis
+    HostPlan plan_;                  // the basis's plan (big tables dropped) plus q
     DevPoint dp_{};
+    size_t own_bytes_ = 0;
     int device_ = 0;
     int sms_ = 0;
     bool simt_ = false;        // FPM_KERNELS=simt: CUDA-core decompose and CRT

@@ -82,7 +82,16 @@ struct CrtConsts {
     uint32_t mhi[kMaxK + 1];    // and high 16 bits
     uint32_t q[kMaxL + 2];      // q, zero above L
 };
-CrtConsts make_crt_consts(const HostPlan& pl);
+// top: the K constants' top limbs M_j[L - 1], then (-P mod q)'s top limb.
+CrtConsts make_crt_consts(const HostPlan& pl, const uint32_t* top);
+
+// The modulus tables of a context on the device (crt_tables.cu): M (K x L),
+// negvP ((K + 1) x L), and for L >= 2 the tensor-core CRT images img (K rows)
+// and img_v (K + 1 rows) of crt_image_bytes each; Pq is scratch of L words.
+// pl needs its basis and q / q_top; pc and q are device copies.
+size_t crt_image_bytes(const HostPlan& pl, int rows);
+void build_crt_tables(const HostPlan& pl, const PrimeConsts* pc, const uint32_t* q, uint32_t* M, uint32_t* negvP,
+                      uint32_t* Pq, uint8_t* img, uint8_t* img_v, cudaStream_t st);
 bool crt_pipe_supported(const DevPoint& d, const uint32_t* Y, uint32_t n_begin, uint32_t n_end);
 void crt_pipe_init_attributes();
 void launch_crt_pipe(const DevPoint& d, const CrtConsts& cc, const uint32_t* Y, uint32_t* c, uint32_t n_begin,

@@ -107,15 +107,41 @@ size_t device_footprint(const HostPlan& pl) {
     return t;
 }
 
-HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2) {
-    if (N < 2 || (N & (N - 1)) || N > (1u << kMaxLogN)) {
-        throw std::runtime_error("unsupported transform length N = " + std::to_string(N) +
-                                 ": expected a power of two from 2 to 2^" + std::to_string(kMaxLogN));
-    }
+int modulus_bits(const uint32_t* q, int L) {
     if (L < 1 || L > kMaxL) {
         throw std::runtime_error("unsupported limb count L = " + std::to_string(L) + ": expected 1 to " +
                                  std::to_string(kMaxL) + " limbs (moduli of up to " + std::to_string(32 * kMaxL) +
                                  " bits)");
+    }
+    const int qbits = bit_length(q, L);
+    if (qbits <= 32 * (L - 1)) {
+        throw std::runtime_error("modulus q has a zero top limb: its " + std::to_string(qbits) +
+                                 " bits fit in fewer than the " + std::to_string(L) + " limbs given");
+    }
+    return qbits;
+}
+
+void check_length(uint32_t N) {
+    if (N < 2 || (N & (N - 1)) || N > (1u << kMaxLogN)) {
+        throw std::runtime_error("unsupported transform length N = " + std::to_string(N) +
+                                 ": expected a power of two from 2 to 2^" + std::to_string(kMaxLogN));
+    }
+}
+
+HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2) {
+    check_length(N);
+    const int qbits = modulus_bits(q, L);
+    HostPlan pl = make_plan_basis(N, W, L, qbits, pmax_log2);
+    set_modulus(pl, q);
+    return pl;
+}
+
+HostPlan make_plan_basis(uint32_t N, uint32_t W, int L, int qbits, int pmax_log2) {
+    check_length(N);
+    if (L < 1 || L > kMaxL || qbits <= 32 * (L - 1) || qbits > 32 * L) {
+        throw std::runtime_error("unsupported modulus: " + std::to_string(qbits) + " bits in L = " +
+                                 std::to_string(L) + " limbs (1 to " + std::to_string(kMaxL) +
+                                 " limbs, nonzero top limb)");
     }
     if (pmax_log2 < 24 || pmax_log2 > 31) throw std::runtime_error("prime window must be 2^24 .. 2^31");
     HostPlan pl;
@@ -127,13 +153,7 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
     uint32_t logN = 0;
     while ((1u << logN) < N) ++logN;
     pl.g = make_geometry(logN);
-    pl.q.assign(q, q + L);
-    const int qbits = bit_length(q, L);
-    if (qbits <= 32 * (L - 1)) {
-        throw std::runtime_error("modulus q has a zero top limb: its " + std::to_string(qbits) +
-                                 " bits fit in fewer than the " + std::to_string(L) + " limbs given");
-    }
-    pl.q_top = modulus_top(q, L);
+    pl.qbits = qbits;
 
     // Primes p = 1 (mod step), step = max(2N, 2^16), from the top of the window
     // downward until sum log2 p > 2 bits(q) + logN + 1 + 20: then |c| < N q^2 is
@@ -284,6 +304,27 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
         }
     }
 
+    if (crt_uses_tc(pl)) {
+        pl.crt_u = (4 * static_cast<uint32_t>(L) - 1 + 31) / 32 * 32;
+        pl.crt_tmem_cols = 32;
+        while (pl.crt_tmem_cols < pl.crt_u) pl.crt_tmem_cols *= 2;
+    }
+    return pl;
+}
+
+void set_modulus_limbs(HostPlan& pl, const uint32_t* q) {
+    const int bits = modulus_bits(q, pl.L);
+    if (bits != pl.qbits) {
+        throw std::runtime_error("modulus of " + std::to_string(bits) + " bits given to a prime basis built for " +
+                                 std::to_string(pl.qbits) + " bits");
+    }
+    pl.q.assign(q, q + pl.L);
+    pl.q_top = modulus_top(q, pl.L);
+}
+
+void set_modulus(HostPlan& pl, const uint32_t* q) {
+    set_modulus_limbs(pl, q);
+    const int K = pl.K, L = pl.L;
     // M_j = prod_{i != j} p_i mod q, P mod q, and negvP_v = (q - v P mod q) mod q
     // for v = 0..K (reference rns_plan.h:224-247).
     pl.M.assign(static_cast<size_t>(K) * L, 0);
@@ -310,9 +351,6 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
 
     // Tensor-core CRT image.
     if (crt_uses_tc(pl)) {
-        pl.crt_u = (4 * static_cast<uint32_t>(L) - 1 + 31) / 32 * 32;
-        pl.crt_tmem_cols = 32;
-        while (pl.crt_tmem_cols < pl.crt_u) pl.crt_tmem_cols *= 2;
         const uint32_t chunks = static_cast<uint32_t>((K + 31) / 32);
         const size_t cchunk = static_cast<size_t>(pl.crt_u) * 128;
         const uint32_t low_bytes = 4 * static_cast<uint32_t>(L - 1);
@@ -341,7 +379,6 @@ HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_lo
         });
         pl.negp_top = pl.negvP[static_cast<size_t>(L) + L - 1];
     }
-    return pl;
 }
 
 }  // namespace fpm

@@ -43,6 +43,7 @@ struct HostPlan {
     uint32_t N = 0, W = 0;
     int L = 0, K = 0;
     Geometry g;
+    int qbits = 0;                // bits of q: the prime basis depends on q only through them
     std::vector<uint32_t> q;      // L
     double q_top = 0;             // top limbs of q as a double
     int pmax_log2 = 30;           // primes below 2^pmax_log2
@@ -117,5 +118,19 @@ size_t device_footprint(const HostPlan& pl);
 // (rns_plan.h:141-153) and uses fully reduced butterflies.
 constexpr int kDefaultPrimeBits = 30;
 HostPlan make_plan(uint32_t N, uint32_t W, const uint32_t* q, int L, int pmax_log2 = kDefaultPrimeBits);
+
+// The plan in two parts.  make_plan_basis builds everything that depends on q
+// only through its bit length -- the prime set, twiddles, decompose constants
+// and images -- so one basis serves every modulus of that width;
+// set_modulus adds q and the tables built from it (M, negvP, the CRT images,
+// negp_top), set_modulus_limbs only q and q_top (for callers that build the
+// rest on the device).  make_plan is make_plan_basis + set_modulus.
+// modulus_bits checks q (L in range, nonzero top limb) and returns its bits;
+// check_length throws unless N is a power of two in [2, 2^kMaxLogN].
+int modulus_bits(const uint32_t* q, int L);
+void check_length(uint32_t N);
+HostPlan make_plan_basis(uint32_t N, uint32_t W, int L, int qbits, int pmax_log2 = kDefaultPrimeBits);
+void set_modulus_limbs(HostPlan& pl, const uint32_t* q);
+void set_modulus(HostPlan& pl, const uint32_t* q);
 
 }  // namespace fpm

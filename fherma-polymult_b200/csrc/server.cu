@@ -63,6 +63,7 @@ Server::Server(const std::vector<Engine*>& points, const ServerConfig& cfg)
         throw std::runtime_error("server: max_batch must be in [1, " + std::to_string(kGroupMax) + "]");
     int dev = -1;
     check(cudaGetDevice(&dev), "cudaGetDevice");
+    device_ = dev;
     for (Engine* e : points_) {
         if (!e) throw std::runtime_error("server: null point");
         if (e->device() != dev) throw std::runtime_error("server: every point must live on the current device");
@@ -115,19 +116,31 @@ Server::~Server() {
     if (base_) cudaFree(base_);
 }
 
-size_t Server::footprint(uint32_t point) const { return footprint_.at(point); }
+size_t Server::footprint(uint32_t point) const {
+    std::lock_guard<std::mutex> lk(mu_);
+    return footprint_.at(point);
+}
+
+uint32_t Server::add_point(Engine* e) {
+    if (!e) throw std::runtime_error("server: null point");
+    if (e->device() != device_) throw std::runtime_error("server: every point must live on the server's device");
+    std::lock_guard<std::mutex> lk(mu_);
+    points_.push_back(e);
+    footprint_.push_back(3 * round_up(e->words() * 4) + 2 * round_up(e->residues() * 4));
+    return static_cast<uint32_t>(points_.size() - 1);
+}
 
 uint64_t Server::submit(uint32_t point, const uint32_t* a, const uint32_t* b, uint32_t* c) {
-    if (point >= points_.size()) throw std::runtime_error("server: point index out of range");
     if (!a || !b || !c) throw std::runtime_error("server: NULL buffer");
-    if (footprint_[point] > arena_.size()) {
-        throw std::runtime_error("server: a request on point " + std::to_string(point) + " needs " +
-                                 std::to_string(footprint_[point]) + " bytes of device memory; the budget is " +
-                                 std::to_string(arena_.size()));
-    }
     uint64_t t;
     {
         std::lock_guard<std::mutex> lk(mu_);
+        if (point >= points_.size()) throw std::runtime_error("server: point index out of range");
+        if (footprint_[point] > arena_.size()) {
+            throw std::runtime_error("server: a request on point " + std::to_string(point) + " needs " +
+                                     std::to_string(footprint_[point]) + " bytes of device memory; the budget is " +
+                                     std::to_string(arena_.size()));
+        }
         t = reqs_.size();
         Request r;
         r.point = point;

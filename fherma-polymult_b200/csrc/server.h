@@ -79,6 +79,10 @@ public:
     void replay(uint32_t n, const uint32_t* point, const double* arrival_us, const uint32_t* const* a,
                 const uint32_t* const* b, uint32_t* const* c, double* latency_us);
 
+    // Adds a point while the server runs (thread-safe); returns its index.
+    // Requests on it may be submitted as soon as this returns.
+    uint32_t add_point(Engine* e);
+
     ServerStats stats() const;
     size_t footprint(uint32_t point) const;
     size_t budget() const { return arena_.size(); }
@@ -107,8 +111,9 @@ private:
     bool reap();
     void launch(Lane& lane);
 
-    std::vector<Engine*> points_;
+    std::vector<Engine*> points_;      // guarded by mu_ (add_point appends)
     std::vector<size_t> footprint_;
+    int device_ = -1;
     ServerConfig cfg_;
     Arena arena_;
     uint8_t* base_ = nullptr;          // device arena

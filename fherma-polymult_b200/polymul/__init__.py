@@ -93,6 +93,9 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
         "fpm_plan_info": ([ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _u32p, ctypes.POINTER(FpmInfo), _u32p],
                           ctypes.c_int),
         "fpm_get_primes": ([vp, _u32p], ctypes.c_int),
+        "fpm_get_crt_tables": ([vp, _u32p, _u32p], ctypes.c_int),
+        "fpm_tune_host_path": ([vp, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+        "fpm_server_add_point": ([vp, vp, ctypes.POINTER(ctypes.c_uint32)], ctypes.c_int),
         "fpm_stage_decompose": ([vp, vp, vp, ctypes.c_int, vp], ctypes.c_int),
         "fpm_stage_transform": ([vp, vp, vp, ctypes.c_int, vp], ctypes.c_int),
         "fpm_stage_crt": ([vp, vp, vp, vp], ctypes.c_int),
@@ -190,6 +193,20 @@ class Context:
         out = np.zeros(self.K, np.uint32)
         _check(self._lib.fpm_get_primes(self._h, out.ctypes.data_as(_u32p)))
         return out
+
+    def tune_host_path(self) -> int:
+        """Measures the host path's copy chunking on this point (as
+        fherma_init does); returns the chunk count kept."""
+        n = ctypes.c_int()
+        _check(self._lib.fpm_tune_host_path(self._h, ctypes.byref(n)))
+        return n.value
+
+    def crt_tables(self) -> tuple[np.ndarray, np.ndarray]:
+        """The CRT constants built on the device: M (K x L), negvP ((K + 1) x L)."""
+        M = np.zeros((self.K, self.L), np.uint32)
+        negvP = np.zeros((self.K + 1, self.L), np.uint32)
+        _check(self._lib.fpm_get_crt_tables(self._h, M.ctypes.data_as(_u32p), negvP.ctypes.data_as(_u32p)))
+        return M, negvP
 
     def run(self, a, b, out=None) -> np.ndarray:
         """c = a b on host arrays (N x L u32)."""
@@ -328,6 +345,13 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+    def add_point(self, ctx) -> int:
+        """Adds a context while the server runs; returns its point index."""
+        idx = ctypes.c_uint32()
+        _check(self._lib.fpm_server_add_point(self._h, ctx.handle, ctypes.byref(idx)))
+        self.contexts.append(ctx)
+        return idx.value
 
     def footprint(self, point: int) -> int:
         out = ctypes.c_uint64()

@@ -69,6 +69,14 @@ FPM_API int fpm_init_ex(uint32_t N, uint32_t W, uint32_t L, const uint32_t* q, i
  * written.  Calls on one context must not overlap. */
 FPM_API int fpm_run(fpm_ctx* ctx, const uint32_t* a, const uint32_t* b, uint32_t* c);
 
+/* Counterpart of the copy-mode measurement in the reference's fherma_init
+ * (solve.cu:805-862): times the host path of fpm_run on this point with 1 to
+ * 4 copy chunks (each candidate 1 + 3 products on the context's own pinned
+ * buffers) and keeps the fastest, the default unless another is 5% faster;
+ * the count is returned in *chunks (may be NULL).  Synchronous.  fherma_init
+ * calls it; without it fpm_run uses the default. */
+FPM_API int fpm_tune_host_path(fpm_ctx* ctx, int* chunks);
+
 /* One product on DEVICE buffers (N x L u32 each), enqueued on `stream` (a
  * cudaStream_t, NULL for the legacy default stream); returns after enqueueing.
  * Calls on one context must be ordered on one stream (they share workspaces). */
@@ -139,6 +147,14 @@ FPM_API int fpm_plan_info_ex(uint32_t N, uint32_t W, uint32_t L, const uint32_t*
 /* The K primes of the RNS basis, in order (same set and order as the
  * reference's make_plan, rns_plan.h:138-153). */
 FPM_API int fpm_get_primes(const fpm_ctx* ctx, uint32_t* out);
+/* The context's CRT constants as built on the device by fpm_init: M_j =
+ * P / p_j mod q (K x L limbs) and negvP_v = -v P mod q ((K + 1) x L), the
+ * tables of the reference's make_plan (rns_plan.h:224-247).  fpm_init builds
+ * them from the prime basis with one short kernel; the q-independent tables
+ * (twiddles, decompose constants) are shared by every context on the device
+ * with the same N, L, bit length of q and prime window, so a context for a new
+ * modulus of a width in use builds and uploads only these. */
+FPM_API int fpm_get_crt_tables(const fpm_ctx* ctx, uint32_t* M, uint32_t* negvP);
 
 /* Stage entry points on device buffers, enqueued on `stream` (no reference
  * counterpart as functions; they expose the reference's kernels' results for
@@ -229,6 +245,12 @@ typedef struct fpm_server_stats {
 
 FPM_API int fpm_server_create(fpm_ctx* const* points, uint32_t count, uint64_t budget_bytes, int lanes,
                               int max_batch, fpm_server** out);
+/* Adds a point to a running server (thread-safe) and returns its index in
+ * *index; requests on it may be submitted at once.  Since the prime-basis
+ * tables are shared across contexts (fpm_get_crt_tables), a context for a new
+ * modulus of a width the server already holds takes little set-up, so new
+ * moduli can join mid-stream.  The context must outlive the server. */
+FPM_API int fpm_server_add_point(fpm_server* srv, fpm_ctx* point, uint32_t* index);
 /* Device bytes one request on `point` takes from the arena. */
 FPM_API int fpm_server_footprint(const fpm_server* srv, uint32_t point, uint64_t* bytes);
 /* Queues a request (thread-safe; returns at once).  FPM_EINVAL if it can

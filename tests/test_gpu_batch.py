@@ -45,12 +45,14 @@ def mixed(cuda):
         c.close()
 
 
-def test_batch_plain_path_matches_oracle_on_small_members(mixed):
+def test_batch_members_match_oracle(mixed):
+    """Every member of the mix, the N = 65536 / 2048-bit ones included, against
+    the oracle (the batch schedules below are then checked against these)."""
     ctxs, ops, expect = mixed
     for ctx, (a, b), e in zip(ctxs, ops, expect):
-        if ctx.N <= 4096:
-            q = oracle_q(ctx)
-            assert np.array_equal(e, oracle.OraclePlan(ctx.N, q).polymul(a, b))
+        q = oracle_q(ctx)
+        bits = 31 if ctx.prime_bits == 31 else 30
+        assert np.array_equal(e, oracle.OraclePlan(ctx.N, q, pmax_log2=bits).polymul(a, b)), (ctx.N, ctx.W)
 
 
 def oracle_q(ctx):
@@ -58,6 +60,27 @@ def oracle_q(ctx):
         if (N, W) == (ctx.N, ctx.W):
             return wl.case(N, W, "uniform", seed=900 + i)[0]
     raise KeyError
+
+
+def test_batch_n65536_members_match_oracle(cuda):
+    """Two N = 65536 products (W = 2048 and 1747) in one batch with the tuned
+    schedule, each against the oracle."""
+    pts = [(65536, 2048), (65536, 1747)]
+    ctxs, qs, ops = [], [], []
+    try:
+        for i, (N, W) in enumerate(pts):
+            q, a, b = wl.case(N, W, "uniform", seed=3100 + i)
+            ctxs.append(polymul.Context(N, W, q))
+            qs.append(q)
+            ops.append((a, b))
+        with polymul.Batch(ctxs) as bt:
+            bt.tune(reps=1)
+            got = bt.run([a for a, _ in ops], [b for _, b in ops])
+        for (N, W), q, (a, b), g in zip(pts, qs, ops, got):
+            assert np.array_equal(g, oracle.OraclePlan(N, q).polymul(a, b)), (N, W)
+    finally:
+        for c in ctxs:
+            c.close()
 
 
 @pytest.mark.parametrize("sched", SCHEDULES, ids=lambda s: "L%d-o%d-g%d-p%d-pipe%d" % s)
