@@ -189,6 +189,54 @@ int enqueue_grouped(const std::vector<GroupedProduct>& prods_, const BatchSchedu
         }
     };
 
+    // Every product of mixed-row-length geometry (R = 64) through each pass in
+    // one launch (layout 3): items as in transform(), any row length.
+    auto transform_mixed = [&](const std::vector<size_t>& list, bool lazy, cudaStream_t s) {
+        struct Item {
+            size_t p;
+            uint32_t j0, nj;
+        };
+        std::vector<Item> items;
+        uint32_t max_log_s = 6;
+        for (size_t i : list) max_log_s = std::max(max_log_s, prods_[i].d.logS);
+        if (sched_.prime_group <= 0) {
+            for (size_t i : list) items.push_back({i, 0, static_cast<uint32_t>(prods_[i].d.K)});
+        } else {
+            const uint32_t grp = static_cast<uint32_t>(sched_.prime_group);
+            for (uint32_t r = 0;; ++r) {
+                bool any = false;
+                for (size_t i : list) {
+                    const uint32_t K = static_cast<uint32_t>(prods_[i].d.K), j0 = r * grp;
+                    if (j0 >= K) continue;
+                    items.push_back({i, j0, std::min(grp, K - j0)});
+                    any = true;
+                }
+                if (!any) break;
+            }
+        }
+        for (int pass : {int(kPassColFwd), int(kPassRow), int(kPassColInv)}) {
+            uint32_t grid = 0;
+            if (sched_.grid > 0) {
+                grid = static_cast<uint32_t>(sched_.grid) * static_cast<uint32_t>(env.sms) *
+                       static_cast<uint32_t>(std::max(1, env.occupancy->at(occupancy_key(pass, 63, max_log_s, lazy))));
+            }
+            fill.reset();
+            auto flush = [&] {
+                if (fill.t->count) {
+                    launch_ntt_mixed(*fill.t, pass, lazy, max_log_s, grid, s);
+                    ++launches_;
+                }
+                fill.reset();
+            };
+            for (const Item& it : items) {
+                if (fill.full()) flush();
+                const GroupedProduct& p = prods_[it.p];
+                fill.add(p.d, p.a, p.b, p.A, p.B, p.c, it.j0, ntt_mixed_blocks(pass, p.d.logS, it.nj));
+            }
+            flush();
+        }
+    };
+
     size_t ev = 0;
     auto fork = [&](cudaStream_t from, cudaStream_t to) {
         check(cudaEventRecord(env.events.at(ev), from), "event record");
@@ -213,6 +261,32 @@ int enqueue_grouped(const std::vector<GroupedProduct>& prods_, const BatchSchedu
         }
         small_ntt(small, st);
         for (cudaStream_t s : used) fork(s, st);
+        crt(all, st);
+    } else if (sched_.layout == 3) {
+        // One launch per stage: grouped decompose, the three transform passes
+        // over every R = 64 product at once (per prime window), grouped CRT.
+        // Other geometries (N <= 2048, N >= 2^18) keep their own launches.
+        decompose(all, st);
+        std::vector<size_t> mixed[2];
+        for (auto& kv : classes) {
+            bool ok = true;
+            for (size_t i : kv.second) ok = ok && ntt_mixed_ok(prods_[i].d);
+            if (ok) {
+                mixed[kv.first.lazy ? 1 : 0].insert(mixed[kv.first.lazy ? 1 : 0].end(), kv.second.begin(),
+                                                    kv.second.end());
+            } else {
+                transform(kv.first, kv.second, st);
+            }
+        }
+        for (int lz = 0; lz < 2; ++lz) {
+            if (mixed[lz].empty()) continue;
+            // Keep the schedule's product order (classes regrouped them).
+            std::vector<size_t> list;
+            for (size_t i : ord)
+                if (std::find(mixed[lz].begin(), mixed[lz].end(), i) != mixed[lz].end()) list.push_back(i);
+            transform_mixed(list, lz == 1, st);
+        }
+        small_ntt(small, st);
         crt(all, st);
     } else {
         size_t b = 0;
@@ -319,7 +393,7 @@ cudaStream_t Batch::branch(size_t i) {
 }
 
 void Batch::set_schedule(const BatchSchedule& s) {
-    if (s.layout < 0 || s.layout > 2 || s.order < 0 || s.order > 1 || s.prime_group < 0 || s.grid < 0 ||
+    if (s.layout < 0 || s.layout > 3 || s.order < 0 || s.order > 1 || s.prime_group < 0 || s.grid < 0 ||
         s.pipe_min_log_n < 0 || s.pipe_min_log_n > 22)
         throw std::runtime_error("batch: invalid schedule");
     sched_ = s;
@@ -350,6 +424,17 @@ void Batch::build_graph() {
             if (pass != kPassRow && p.d.logR == 0) continue;
             const uint64_t k = occupancy_key(pass, p.d.logR, p.d.logS, p.d.lazy != 0);
             if (!occupancy_.count(k)) occupancy_[k] = ntt_group_occupancy(pass, p.d.logR, p.d.logS, p.d.lazy != 0);
+        }
+    }
+    // The mixed-geometry kernels (layout 3), keyed by the largest row length.
+    uint32_t max_log_s[2] = {0, 0};
+    for (const GroupedProduct& p : prods_)
+        if (ntt_mixed_ok(p.d)) max_log_s[p.d.lazy ? 1 : 0] = std::max(max_log_s[p.d.lazy ? 1 : 0], p.d.logS);
+    for (int lz = 0; lz < 2; ++lz) {
+        if (!max_log_s[lz]) continue;
+        for (int pass : {int(kPassColFwd), int(kPassRow), int(kPassColInv)}) {
+            const uint64_t k = occupancy_key(pass, 63, max_log_s[lz], lz == 1);
+            if (!occupancy_.count(k)) occupancy_[k] = ntt_mixed_occupancy(pass, lz == 1, max_log_s[lz]);
         }
     }
     for (size_t i = 0; i < classes; ++i) branch(i);
@@ -452,7 +537,7 @@ uint32_t Batch::take_error() {
 double Batch::tune(int reps) {
     if (reps < 1) reps = 1;
     std::vector<BatchSchedule> cands;
-    for (int layout : {0, 1, 2})
+    for (int layout : {0, 1, 2, 3})
         for (int grp : {0, 16})
             for (int grid : {0, 1})
                 for (int pipe : {0, 14, 16}) cands.push_back(BatchSchedule{layout, 1, grp, grid, pipe});

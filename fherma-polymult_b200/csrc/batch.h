@@ -28,7 +28,9 @@ namespace fpm {
 
 struct BatchSchedule {
     int layout = 1;        // 0 one stream; 1 geometry chains as branches between the shared
-                           // decompose and CRT; 2 a whole branch (decompose .. CRT) per geometry
+                           // decompose and CRT; 2 a whole branch (decompose .. CRT) per geometry;
+                           // 3 one launch per stage: each transform pass covers every R = 64
+                           // product whatever its row length (mixed-geometry kernels)
     int order = 1;         // 0 products as given; 1 largest first
     int prime_group = 0;   // primes per transform item; 0 = all of a product's primes
     int grid = 0;          // transform grids: 0 one block per tile; k > 0 persistent,

@@ -127,5 +127,13 @@ void launch_crt_tc_group(const GroupTable& t, cudaStream_t st);
 void launch_ntt_group(const GroupTable& t, int pass, uint32_t logR, uint32_t logS, bool lazy, uint32_t grid,
                       cudaStream_t st);
 int ntt_group_occupancy(int pass, uint32_t logR, uint32_t logS, bool lazy);
+// The same over items of mixed row lengths (R = 64 each, logS <= max_log_s):
+// one launch per pass whatever the geometries; blocks per item from
+// ntt_mixed_blocks (the row pass runs two 128-thread tiles per block for
+// 16-element rounds).
+bool ntt_mixed_ok(const DevPoint& d);
+uint32_t ntt_mixed_blocks(int pass, uint32_t logS, uint32_t primes);
+void launch_ntt_mixed(const GroupTable& t, int pass, bool lazy, uint32_t max_log_s, uint32_t grid, cudaStream_t st);
+int ntt_mixed_occupancy(int pass, bool lazy, uint32_t max_log_s);
 
 }  // namespace fpm

@@ -43,38 +43,54 @@ using RP = Rounds<NSUB, XS, SWZ, RB>;
 template <int RB>
 using SwzC = std::conditional_t<RB == 3, SwzCol, SwzRow>;
 
+// The threads that own one tile: the whole block, or one 128-thread half of a
+// 256-thread block (the grouped row pass of mixed geometries runs two
+// 128-thread tiles per block).
+struct BlockTeam {
+    static __device__ __forceinline__ uint32_t tid() { return threadIdx.x; }
+    static __device__ __forceinline__ void sync() { __syncthreads(); }
+};
+struct HalfTeam {
+    static __device__ __forceinline__ uint32_t tid() { return threadIdx.x & 127u; }
+    static __device__ __forceinline__ void sync() {
+        asm volatile("bar.sync %0, 128;" ::"r"(1u + (threadIdx.x >> 7)) : "memory");
+    }
+};
+
 // Round R through shared memory on NV tiles.
-template <int NSUB, int XS, class SWZ, int RB, int R, bool LAZY, int NV, class TW>
+template <int NSUB, int XS, class SWZ, int RB, int R, bool LAZY, int NV, class TEAM = BlockTeam, class TW>
 __device__ __forceinline__ void fwd_step(uint32_t* const (&tiles)[NV], const TW& tw, uint32_t p) {
-    const uint32_t base = round_base<NSUB, XS, SWZ, RB, R>(threadIdx.x);
+    const uint32_t base = round_base<NSUB, XS, SWZ, RB, R>(TEAM::tid());
     uint32_t v[NV][1 << RB];
 #pragma unroll
     for (int o = 0; o < NV; ++o) load_round<NSUB, XS, SWZ, RB, R>(tiles[o], v[o], base);
     fwd_round<NSUB, XS, SWZ, RB, R, LAZY, NV>(v, base, tw, p);
 #pragma unroll
     for (int o = 0; o < NV; ++o) store_round<NSUB, XS, SWZ, RB, R>(tiles[o], v[o], base);
-    __syncthreads();
+    TEAM::sync();
 }
 
-template <int NSUB, int XS, class SWZ, int RB, int R, int REND, bool LAZY, int NV, class TW>
+template <int NSUB, int XS, class SWZ, int RB, int R, int REND, bool LAZY, int NV, class TEAM = BlockTeam,
+          class TW>
 __device__ __forceinline__ void fwd_range(uint32_t* const (&tiles)[NV], const TW& tw, uint32_t p) {
     if constexpr (R < REND) {
-        fwd_step<NSUB, XS, SWZ, RB, R, LAZY, NV>(tiles, tw, p);
-        fwd_range<NSUB, XS, SWZ, RB, R + 1, REND, LAZY, NV>(tiles, tw, p);
+        fwd_step<NSUB, XS, SWZ, RB, R, LAZY, NV, TEAM>(tiles, tw, p);
+        fwd_range<NSUB, XS, SWZ, RB, R + 1, REND, LAZY, NV, TEAM>(tiles, tw, p);
     }
 }
 
 // Inverse rounds R, R - 1, ..., RLO through shared memory.
-template <int NSUB, int XS, class SWZ, int RB, int R, int RLO, bool LAZY, bool NEG, class TW>
+template <int NSUB, int XS, class SWZ, int RB, int R, int RLO, bool LAZY, bool NEG, class TEAM = BlockTeam,
+          class TW>
 __device__ __forceinline__ void inv_range(uint32_t* tile, const TW& tw, uint32_t p) {
     if constexpr (R >= RLO) {
-        const uint32_t base = round_base<NSUB, XS, SWZ, RB, R>(threadIdx.x);
+        const uint32_t base = round_base<NSUB, XS, SWZ, RB, R>(TEAM::tid());
         uint32_t v[1 << RB];
         load_round<NSUB, XS, SWZ, RB, R>(tile, v, base);
         inv_round<NSUB, XS, SWZ, RB, R, LAZY, NEG>(v, base, tw, p);
         store_round<NSUB, XS, SWZ, RB, R>(tile, v, base);
-        __syncthreads();
-        inv_range<NSUB, XS, SWZ, RB, R - 1, RLO, LAZY, NEG>(tile, tw, p);
+        TEAM::sync();
+        inv_range<NSUB, XS, SWZ, RB, R - 1, RLO, LAZY, NEG, TEAM>(tile, tw, p);
     }
 }
 
@@ -457,10 +473,11 @@ constexpr size_t row_bar_offset() {
 
 // phase: parity of this tile's use of the tables barrier (the block's tile
 // count so far, mod 2); the barrier is initialised by the kernel.
-template <int LOGS, bool LAZY>
+// smem: this team's region (row_smem_t<LOGS>() bytes, 1024-byte aligned);
+// tbar: its tables barrier (initialised, count 1).
+template <int LOGS, bool LAZY, class TEAM = BlockTeam>
 __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, int j, uint32_t bx,
-                                         uint32_t phase) {
-    extern __shared__ __align__(1024) uint32_t smem[];
+                                         uint32_t phase, uint32_t* smem, uint64_t* tbar) {
     using RG = RowGeom<LOGS>;
     constexpr int RB = row_pass_rb(LOGS), E = 1 << RB, T = ntt_threads<RB>();
     using RPR = RP<LOGS, 0, SwzRow, RB>;
@@ -479,12 +496,11 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
     const RowTable<LOGS, RG::kStride, true, RG::kFlip> iw{tf};
     uint32_t* const tiles[2] = {ta, tb};
 
-    uint64_t* tbar = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(smem) + row_bar_offset<LOGS>());
     // The tables stream into shared memory while round 0 loads its elements.
-    if (threadIdx.x < 32) row_tables_bulk<LOGS>(tf, d, j, u0, tbar);
+    if (TEAM::tid() < 32) row_tables_bulk<LOGS>(tf, d, j, u0, tbar);
     // Round 0 straight from global memory (the thread's E elements lie in one row).
     {
-        const uint32_t base = round_base<LOGS, 0, SwzRow, RB, 0>(threadIdx.x);
+        const uint32_t base = round_base<LOGS, 0, SwzRow, RB, 0>(TEAM::tid());
         constexpr int sh = RPR::lo(0);
         const size_t at = row_offset<LOGS>(base, u0, R);
         uint32_t v[2][E];
@@ -495,17 +511,17 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
         }
         // The bound only guards against a copy that never lands: past it the
         // error word gets bit 2 and the block goes on (with wrong twiddles).
-        if (!tc::wait_parity(tbar, phase, d.wait_ns) && (threadIdx.x & 31) == 0) atomicOr(d.err, 4u);
+        if (!tc::wait_parity(tbar, phase, d.wait_ns) && (TEAM::tid() & 31) == 0) atomicOr(d.err, 4u);
         fwd_round<LOGS, 0, SwzRow, RB, 0, LAZY, 2>(v, base, fw, p);
 #pragma unroll
         for (int o = 0; o < 2; ++o) store_round<LOGS, 0, SwzRow, RB, 0>(tiles[o], v[o], base);
-        __syncthreads();
+        TEAM::sync();
     }
-    fwd_range<LOGS, 0, SwzRow, RB, 1, last, LAZY, 2>(tiles, fw, p);
+    fwd_range<LOGS, 0, SwzRow, RB, 1, last, LAZY, 2, TEAM>(tiles, fw, p);
     // Last forward round, the pointwise product and the first inverse round in
     // registers.
     {
-        const uint32_t base = round_base<LOGS, 0, SwzRow, RB, last>(threadIdx.x);
+        const uint32_t base = round_base<LOGS, 0, SwzRow, RB, last>(TEAM::tid());
         uint32_t v[2][E];
         load_round<LOGS, 0, SwzRow, RB, last>(ta, v[0], base);
         load_round<LOGS, 0, SwzRow, RB, last>(tb, v[1], base);
@@ -520,8 +536,8 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
             }
             store_round<LOGS, 0, SwzRow, RB, last>(ta, v[0], base);
             store_round<LOGS, 0, SwzRow, RB, last>(tb, v[1], base);
-            __syncthreads();
-            for (uint32_t i = threadIdx.x; i < 2048; i += T) {
+            TEAM::sync();
+            for (uint32_t i = TEAM::tid(); i < 2048; i += T) {
                 const size_t at = row_offset<LOGS>(i, u0, R);
                 a[at] = ta[SwzRow::f(i)];
                 b[at] = tb[SwzRow::f(i)];
@@ -540,12 +556,12 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
         }
         inv_round<LOGS, 0, SwzRow, RB, last, LAZY, true>(v[0], base, iw, p);
         store_round<LOGS, 0, SwzRow, RB, last>(ta, v[0], base);
-        __syncthreads();
+        TEAM::sync();
     }
-    inv_range<LOGS, 0, SwzRow, RB, last - 1, 1, LAZY, true>(ta, iw, p);
+    inv_range<LOGS, 0, SwzRow, RB, last - 1, 1, LAZY, true, TEAM>(ta, iw, p);
     // Inverse round 0 straight to global memory.
     {
-        const uint32_t base = round_base<LOGS, 0, SwzRow, RB, 0>(threadIdx.x);
+        const uint32_t base = round_base<LOGS, 0, SwzRow, RB, 0>(TEAM::tid());
         constexpr int sh = RPR::lo(0);
         uint32_t v[E];
         load_round<LOGS, 0, SwzRow, RB, 0>(ta, v, base);
@@ -624,7 +640,7 @@ __global__ void __launch_bounds__(row_threads<LOGS>(), (row_min_blocks<LOGS>()))
     __syncthreads();
     pdl_launch_dependents();
     pdl_wait();
-    row_body<LOGS, LAZY>(d, A, B, mode, blockIdx.y, blockIdx.x, 0);
+    row_body<LOGS, LAZY>(d, A, B, mode, blockIdx.y, blockIdx.x, 0, smem, tbar);
 }
 
 // Grouped launches over products of one geometry class: a (possibly
@@ -672,7 +688,94 @@ __global__ void __launch_bounds__(row_threads<LOGS>(), (row_min_blocks<LOGS>()))
         const uint32_t i = group_locate(t, b);
         const GroupItem& it = t.item[i];
         const uint32_t local = b - t.first[i], per = row_blocks<LOGS>(it.d.logR);
-        row_body<LOGS, LAZY>(it.d, it.A, it.B, kRowProduct, it.j0 + local / per, local % per, n & 1);
+        row_body<LOGS, LAZY>(it.d, it.A, it.B, kRowProduct, it.j0 + local / per, local % per, n & 1, smem, tbar);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Grouped passes over products of mixed row lengths (every item R = 64:
+// N = 2^12 .. 2^17, one prime window): one launch per pass for a whole batch.
+// The column passes switch on the item's row length; the row pass runs
+// 256-thread blocks, one tile per block for 8-element rounds and two
+// 128-thread tiles per block (HalfTeam, named barriers, a shared-memory region
+// and tables barrier each) for 16-element rounds.
+
+template <class F>
+__device__ __forceinline__ void with_row_log(uint32_t logS, F&& f) {
+    switch (logS) {
+        case 6: f(std::integral_constant<int, 6>{}); break;
+        case 7: f(std::integral_constant<int, 7>{}); break;
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        case 9: f(std::integral_constant<int, 9>{}); break;
+        case 10: f(std::integral_constant<int, 10>{}); break;
+        default: f(std::integral_constant<int, 11>{}); break;
+    }
+}
+
+template <bool LAZY>
+__global__ void __launch_bounds__(256, 6) k_ntt_col_fwd_mixed(const __grid_constant__ GroupTable t) {
+    for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
+        if (b != blockIdx.x) __syncthreads();
+        const uint32_t i = group_locate(t, b);
+        const GroupItem& it = t.item[i];
+        const uint32_t local = b - t.first[i], per = (1u << it.d.logS) >> 5;
+        with_row_log(it.d.logS, [&](auto ls) {
+            col_fwd_body<6, decltype(ls)::value, LAZY>(it.d, it.A, it.B, it.j0 + local / per, local % per);
+        });
+    }
+}
+
+template <bool LAZY>
+__global__ void __launch_bounds__(256, 6) k_ntt_col_inv_mixed(const __grid_constant__ GroupTable t) {
+    for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
+        if (b != blockIdx.x) __syncthreads();
+        const uint32_t i = group_locate(t, b);
+        const GroupItem& it = t.item[i];
+        const uint32_t local = b - t.first[i], per = (1u << it.d.logS) >> 5;
+        with_row_log(it.d.logS, [&](auto ls) {
+            col_inv_body<6, decltype(ls)::value, LAZY>(it.d, it.A, it.j0 + local / per, local % per);
+        });
+    }
+}
+
+// Shared memory: two regions of `region` bytes, each ending in its tables
+// barrier.  Block b of item i: tile local(b) (one per block) or tiles
+// 2 local(b) + half (two per block), tile = (prime, row block).
+template <bool LAZY>
+__global__ void __launch_bounds__(256, 3) k_ntt_row_mixed(const __grid_constant__ GroupTable t, uint32_t region) {
+    extern __shared__ __align__(1024) uint32_t smem[];
+    uint8_t* base = reinterpret_cast<uint8_t*>(smem);
+    uint64_t* tbar[2] = {reinterpret_cast<uint64_t*>(base + region - 16),
+                         reinterpret_cast<uint64_t*>(base + 2 * region - 16)};
+    if (threadIdx.x == 0) {
+        tc::mbar_init(tbar[0], 1);
+        tc::mbar_init(tbar[1], 1);
+        tc::fence_mbar_init();
+    }
+    __syncthreads();
+    uint32_t uses[2] = {0, 0};   // every thread counts both regions' uses
+    const uint32_t half = threadIdx.x >> 7;
+    for (uint32_t b = blockIdx.x; b < t.total; b += gridDim.x) {
+        if (b != blockIdx.x) __syncthreads();
+        const uint32_t i = group_locate(t, b);
+        const GroupItem& it = t.item[i];
+        const uint32_t local = b - t.first[i];
+        with_row_log(it.d.logS, [&](auto ls) {
+            constexpr int LS = decltype(ls)::value;
+            const uint32_t per = row_blocks<LS>(6);
+            if constexpr (row_threads<LS>() == 256) {
+                row_body<LS, LAZY, BlockTeam>(it.d, it.A, it.B, kRowProduct, it.j0 + local / per, local % per,
+                                              uses[0] & 1, smem, tbar[0]);
+                ++uses[0];
+            } else {
+                const uint32_t tile = 2 * local + half;
+                row_body<LS, LAZY, HalfTeam>(it.d, it.A, it.B, kRowProduct, it.j0 + tile / per, tile % per,
+                                             uses[half] & 1, reinterpret_cast<uint32_t*>(base + half * region),
+                                             tbar[half]);
+                ++uses[0];
+                ++uses[1];
+            }
+        });
     }
 }
 
@@ -941,6 +1044,86 @@ void launch_ntt_t(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStr
 
 }  // namespace
 
+bool ntt_mixed_ok(const DevPoint& d) { return d.logN > kSmallLogN && d.logR == 6 && d.logS >= 6 && d.logS <= 11; }
+
+uint32_t ntt_mixed_blocks(int pass, uint32_t logS, uint32_t primes) {
+    if (pass != kPassRow) return primes * ((1u << logS) >> 5);
+    uint32_t per = 0, threads = 0;
+    with_log(logS, [&](auto ls) {
+        constexpr int LS = decltype(ls)::value;
+        per = row_blocks<LS>(6);
+        threads = row_threads<LS>();
+    });
+    return threads == 256 ? primes * per : primes * per / 2;
+}
+
+namespace {
+
+uint32_t row_mixed_region(uint32_t max_log_s) {
+    size_t r = 0;
+    for (uint32_t ls = 6; ls <= max_log_s && ls <= 11; ++ls) {
+        with_log(ls, [&](auto l) { r = std::max(r, row_smem_t<decltype(l)::value>()); });
+    }
+    return static_cast<uint32_t>((r + 1023) / 1024 * 1024);
+}
+
+template <bool LAZY>
+void mixed_pass(const GroupTable* t, int pass, uint32_t max_log_s, uint32_t grid, cudaStream_t st, int* occupancy) {
+    auto run = [&](auto kernel, size_t smem, auto... extra) {
+        if (occupancy) {
+            check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy, kernel, 256, smem), "occupancy");
+        } else {
+            kernel<<<grid, 256, smem, st>>>(*t, extra...);
+        }
+    };
+    if (pass == kPassColFwd) {
+        run(k_ntt_col_fwd_mixed<LAZY>, col_fwd_smem_t(6));
+    } else if (pass == kPassColInv) {
+        run(k_ntt_col_inv_mixed<LAZY>, col_inv_smem_t(6));
+    } else if (pass == kPassRow) {
+        const uint32_t region = row_mixed_region(max_log_s);
+        run(k_ntt_row_mixed<LAZY>, 2 * size_t(region), region);
+    } else {
+        throw std::runtime_error("mixed transform: unknown pass");
+    }
+}
+
+template <bool LAZY>
+void mixed_attrs() {
+    check(cudaFuncSetAttribute(k_ntt_col_fwd_mixed<LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(col_fwd_smem_t(6))),
+          "mixed smem");
+    check(cudaFuncSetAttribute(k_ntt_col_inv_mixed<LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(col_inv_smem_t(6))),
+          "mixed smem");
+    check(cudaFuncSetAttribute(k_ntt_row_mixed<LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(2 * row_mixed_region(11))),
+          "mixed smem");
+}
+
+}  // namespace
+
+void launch_ntt_mixed(const GroupTable& t, int pass, bool lazy, uint32_t max_log_s, uint32_t grid, cudaStream_t st) {
+    if (t.total == 0) return;
+    if (grid == 0 || grid > t.total) grid = t.total;
+    if (lazy) {
+        mixed_pass<true>(&t, pass, max_log_s, grid, st, nullptr);
+    } else {
+        mixed_pass<false>(&t, pass, max_log_s, grid, st, nullptr);
+    }
+    check(cudaGetLastError(), "mixed transform launch");
+}
+
+int ntt_mixed_occupancy(int pass, bool lazy, uint32_t max_log_s) {
+    int n = 0;
+    if (lazy) {
+        mixed_pass<true>(nullptr, pass, max_log_s, 0, nullptr, &n);
+    } else {
+        mixed_pass<false>(nullptr, pass, max_log_s, 0, nullptr, &n);
+    }
+    return n;
+}
+
 void build_row_tables(const DevPoint& d, uint2* out, cudaStream_t st) {
     k_row_tables<<<dim3(1u << d.logR, d.K), 256, 0, st>>>(d, out);
     check(cudaGetLastError(), "row tables launch");
@@ -949,6 +1132,8 @@ void build_row_tables(const DevPoint& d, uint2* out, cudaStream_t st) {
 void ntt_init_attributes() {
     attrs_all<true>();
     attrs_all<false>();
+    mixed_attrs<true>();
+    mixed_attrs<false>();
     check(cudaFuncSetAttribute(k_ntt_small, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 1024 * 4),
           "small smem");
 }

@@ -189,7 +189,9 @@ typedef struct fpm_batch fpm_batch;
 typedef struct fpm_batch_info {
     uint32_t count;        /* products */
     int32_t layout;        /* 0 one stream; 1 transform geometries as parallel graph
-                              branches; 2 a whole branch per geometry */
+                              branches; 2 a whole branch per geometry; 3 one launch per
+                              stage (every transform pass covers all products with
+                              N = 2^12 .. 2^17 in one launch, whatever their lengths) */
     int32_t order;         /* 0 as given; 1 largest product first */
     int32_t prime_group;   /* primes per transform work item (0: all of a product's) */
     int32_t grid;          /* transform grids: 0 one block per tile, k > 0 persistent */

@@ -22,7 +22,8 @@ MIXED = [(65536, 2048, 0), (32768, 868, 0), (16384, 512, 0), (8192, 1747, 0), (4
 
 # (layout, order, prime_group, grid, pipe_min_log_n)
 SCHEDULES = [(0, 1, 0, 0, 0), (1, 1, 0, 0, 0), (2, 1, 0, 0, 0), (1, 0, 16, 1, 0), (2, 1, 16, 2, 0), (0, 0, 8, 1, 0),
-             (1, 1, 3, 0, 0), (1, 1, 0, 0, 11), (2, 0, 16, 1, 12), (0, 1, 0, 0, 16)]
+             (1, 1, 3, 0, 0), (1, 1, 0, 0, 11), (2, 0, 16, 1, 12), (0, 1, 0, 0, 16), (3, 1, 0, 0, 0), (3, 0, 16, 1, 0),
+             (3, 1, 5, 2, 16)]
 
 
 @pytest.fixture(scope="module")
@@ -102,7 +103,7 @@ def test_batch_tune_keeps_results(mixed):
     with polymul.Batch(ctxs) as bt:
         bt.run([a for a, _ in ops], [b for _, b in ops])
         info = bt.tune(reps=2)
-        assert info.tuned_us > 0 and 0 <= info.layout <= 2
+        assert info.tuned_us > 0 and 0 <= info.layout <= 3
         got = bt.run([a for a, _ in ops], [b for _, b in ops])
         for g, e in zip(got, expect):
             assert np.array_equal(g, e)
@@ -153,7 +154,7 @@ def test_batch_errors(cuda):
     with polymul.Context(4096, 128, q) as ctx:
         with polymul.Batch([ctx]) as bt:
             with pytest.raises(polymul.FpmError) as e:
-                bt.set_schedule(3, 1, 0, 0)
+                bt.set_schedule(4, 1, 0, 0)
             with pytest.raises(polymul.FpmError):
                 bt.set_schedule(1, 1, 0, 0, 40)
             assert e.value.code == polymul.FPM_EINVAL
