@@ -16,25 +16,25 @@
 // Organisation on the B200: one CTA per SM walks tiles of 128 coefficients
 // (one MMA M); tile i of a CTA accumulates into TMEM buffer i % 2 (256 columns
 // each), so a tile's epilogue overlaps the next tile's staging and MMAs:
-//   * warp 0 (one thread) streams the constant image, chunk by chunk (32
-//     primes, U x 128 bytes), through a two-slot ring (bulk copies, L2-resident);
-//   * warp 2 (one thread) streams y through a three-slot ring with 2-D TMA
-//     copies: per chunk a box of 32 primes x 128 coefficients (16 KB) of the
-//     prime-major K x N array;
+//   * the constant image (U x 128 bytes per chunk of 32 primes, the last chunk
+//     cut to the K steps it uses) is loaded once per CTA by bulk copies and
+//     stays resident in shared memory, so the MMAs never wait for constants;
+//   * warp 2 (one thread) streams y through a ring of 16 KB stages (as many as
+//     shared memory holds beside the constants, 2 to 4) with 2-D TMA copies:
+//     per chunk a box of 32 primes x 128 coefficients of the prime-major
+//     K x N array;
 //   * warps 3-6, one thread per row, read their row's 32 values of a chunk from
 //     the ring (conflict-free), write them in the MMA's K-major byte layout
 //     (two-slot A ring), add up the rounding sum and the top limb, and put v in
 //     the last chunk;
-//   * warp 1 (one thread) issues a chunk's MMAs as soon as its A and B slots
-//     are full;
+//   * warp 1 (one thread) issues a chunk's MMAs as soon as its A slot is full;
 //   * warps 7-10 and 11-14 are two epilogue groups, one per TMEM buffer, one
 //     thread per row: a quotient estimate e from the top TMEM columns (within
 //     one of floor(X / q)), then one pass from the bottom limb up that
-//     assembles X from D with carries, subtracts e q, and tracks the borrows
-//     that tell whether X - e q lies in [0, q); the rare row that does not
-//     (about 2^-11 of them) adds or subtracts q in a second pass over its
-//     staged limbs.  Rows are staged in padded shared memory and a group copies
-//     its tile's 128 rows (one contiguous run of c) out with coalesced stores.
+//     assembles X from D with carries, subtracts e q, stores the limbs of its
+//     row and tracks the borrows that tell whether X - e q lies in [0, q); the
+//     rare row that does not (about 2^-11 of them) adds or subtracts q in a
+//     second pass over what it stored.
 // Per-prime constants and q come from kernel parameters (constant bank).
 // The kernel is compiled for the common limb counts (L = 64, 55, 28, 8) and
 // once for any L.
@@ -53,77 +53,83 @@ namespace fpm {
 namespace {
 
 constexpr int kThreads = 480;             // 15 warps
-constexpr int kBWarp = 0;
 constexpr int kMmaWarp = 1;
 constexpr int kYWarp = 2;
 constexpr int kStagerWarp0 = 3;           // warps 3-6
 constexpr int kEpiWarp0 = 7;              // warps 7-10 (group 0), 11-14 (group 1)
-constexpr uint32_t kCrtTile = 128;           // coefficients per tile
+constexpr uint32_t kCrtTile = 128;        // coefficients per tile
 constexpr uint32_t kChunk = 32;           // K rows (primes) per chunk
 constexpr int kMaxChunks = kMaxK / kChunk;   // K + 1 <= kMaxK rows
-constexpr int kYStages = 3;
-constexpr uint32_t kBSlot = 32768;        // U <= 256 rows of 128 bytes
+constexpr int kMaxYStages = 4;
 constexpr uint32_t kASlot = 16384;        // [8 core columns][128 rows][16 bytes]
 constexpr uint32_t kYSlot = kChunk * kCrtTile * 4;   // [32 primes][128 coefficients] u32
 constexpr int kX = kMaxL + 2;
+constexpr size_t kSmemLimit = 227 * 1024;
 
-// Words per staged result row: a 16-byte-chunk stride that is odd (vector
-// rows, L a multiple of 4) or an odd word stride (scalar rows), so the
-// epilogue's row writes and the copy-out's reads are free of bank conflicts.
-__host__ __device__ constexpr int out_stride(int L) { return (L & 3) == 0 ? 4 * ((L / 4) | 1) : (L | 1); }
-constexpr int kMaxOutStride = out_stride(kMaxL);
+// Shared-memory plan, the same on host and device: the resident constants
+// from 0, then the A ring, the y ring, the per-tile top-limb words and the
+// barriers.
+struct Layout {
+    uint32_t b_bytes;      // resident constant image
+    uint32_t ystages;      // y ring depth
+    __host__ __device__ size_t a_off() const { return (size_t(b_bytes) + 1023) / 1024 * 1024; }
+    __host__ __device__ size_t y_off() const { return a_off() + 2 * size_t(kASlot); }
+    __host__ __device__ size_t meta_off() const { return y_off() + ystages * size_t(kYSlot); }
+    __host__ __device__ size_t bar_off() const { return meta_off() + 2 * kCrtTile * sizeof(uint4); }
+    __host__ __device__ size_t bytes() const { return bar_off() + 32 * 8 + 16; }
+};
 
-constexpr size_t kBOff = 0;
-constexpr size_t kAOff = kBOff + 2 * size_t(kBSlot);
-constexpr size_t kYOff = kAOff + 2 * size_t(kASlot);
-constexpr size_t kMetaOff = kYOff + kYStages * size_t(kYSlot);
-constexpr size_t kOutOff = kMetaOff + 2 * kCrtTile * sizeof(uint4);
-constexpr size_t kBarOff = kOutOff + 2 * size_t(kCrtTile) * kMaxOutStride * 4;
-constexpr int kBars = 2 + 2 + 2 + 2 + 2 * kYStages + 2 + 2 + 2 + 2 + 2;
-constexpr size_t kSmemBytes = kBarOff + kBars * 8 + 16;
-static_assert(kSmemBytes <= 227 * 1024, "shared memory budget");
+// Bytes of the constant image the MMAs read: full chunks of U x 128 bytes,
+// the last one cut to the K steps (8 rows each) its K + 1 - 32 (nch - 1) rows
+// need (a prefix of the chunk: 2 core columns of U x 16 bytes per step).
+__host__ __device__ inline uint32_t resident_b_bytes(int K, uint32_t U) {
+    const int nch = (K + 1 + static_cast<int>(kChunk) - 1) / static_cast<int>(kChunk);
+    const int last_rows = K + 1 - static_cast<int>(kChunk) * (nch - 1);
+    const uint32_t last_steps = static_cast<uint32_t>(last_rows + 7) / 8;
+    return static_cast<uint32_t>(nch - 1) * U * 128 + last_steps * 2 * U * 16;
+}
+
+Layout make_layout(int K, uint32_t U) {
+    Layout l{resident_b_bytes(K, U), kMaxYStages};
+    while (l.ystages > 2 && l.bytes() > kSmemLimit) --l.ystages;
+    return l;
+}
 
 struct Smem {
-    uint8_t* b;          // [2][kBSlot]
+    uint8_t* b;          // resident constant image
     uint8_t* a;          // [2][kASlot]
-    uint32_t* y;         // [kYStages][32][128]
+    uint32_t* y;         // [ystages][32][128]
     uint4* meta;         // [2][128] {top-limb words 0, 1, 2, -}
-    uint32_t* outs;      // [2 groups][128 rows][out_stride(L)] result limbs
-    uint64_t* b_full;    // [2] constant chunk landed
-    uint64_t* b_empty;   // [2] its MMAs finished
+    uint64_t* b_full;    // [1] the constant image landed
     uint64_t* a_full;    // [2] 128 rows staged
     uint64_t* a_empty;   // [2] its MMAs finished
-    uint64_t* y_full;    // [kYStages] TMA box landed
-    uint64_t* y_empty;   // [kYStages] 128 rows read it
+    uint64_t* y_full;    // [kMaxYStages] TMA box landed
+    uint64_t* y_empty;   // [kMaxYStages] 128 rows read it
     uint64_t* d_full;    // [2] a tile's MMAs finished (per TMEM buffer)
     uint64_t* d_empty;   // [2] its epilogue group has read TMEM
     uint64_t* m_full;    // [2] a tile's top-limb words staged
     uint64_t* m_empty;   // [2] and read
-    uint64_t* o_sync;    // [2] per-group barrier (128 arrivals)
     uint32_t* tmem_base;
     volatile uint32_t* abort;
 };
 
-__device__ inline Smem carve(uint8_t* base) {
+__device__ inline Smem carve(uint8_t* base, const Layout& lay) {
     Smem s;
-    s.b = base + kBOff;
-    s.a = base + kAOff;
-    s.y = reinterpret_cast<uint32_t*>(base + kYOff);
-    s.meta = reinterpret_cast<uint4*>(base + kMetaOff);
-    s.outs = reinterpret_cast<uint32_t*>(base + kOutOff);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(base + kBarOff);
+    s.b = base;
+    s.a = base + lay.a_off();
+    s.y = reinterpret_cast<uint32_t*>(base + lay.y_off());
+    s.meta = reinterpret_cast<uint4*>(base + lay.meta_off());
+    uint64_t* bars = reinterpret_cast<uint64_t*>(base + lay.bar_off());
     s.b_full = bars;
-    s.b_empty = bars + 2;
-    s.a_full = bars + 4;
-    s.a_empty = bars + 6;
-    s.y_full = bars + 8;
-    s.y_empty = bars + 8 + kYStages;
-    s.d_full = bars + 8 + 2 * kYStages;
+    s.a_full = bars + 1;
+    s.a_empty = bars + 3;
+    s.y_full = bars + 5;
+    s.y_empty = bars + 5 + kMaxYStages;
+    s.d_full = bars + 5 + 2 * kMaxYStages;
     s.d_empty = s.d_full + 2;
     s.m_full = s.d_full + 4;
     s.m_empty = s.d_full + 6;
-    s.o_sync = s.d_full + 8;
-    s.tmem_base = reinterpret_cast<uint32_t*>(bars + kBars);
+    s.tmem_base = reinterpret_cast<uint32_t*>(bars + 32);
     s.abort = s.tmem_base + 1;
     return s;
 }
@@ -143,36 +149,46 @@ __device__ __forceinline__ void tmem_wait(uint32_t (&r)[16]) {
 template <int LT>
 __global__ void __launch_bounds__(kThreads, 1)
     k_crt_pipe(DevPoint d, const __grid_constant__ CrtConsts cc, const __grid_constant__ CUtensorMap tmY,
-               uint32_t* __restrict__ C, uint32_t n_begin, uint32_t n_end) {
+               uint32_t* __restrict__ C, uint32_t n_begin, uint32_t n_end, Layout lay) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     pdl_launch_dependents();
-    const Smem sm = carve(smem_raw);
+    const Smem sm = carve(smem_raw, lay);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int L = LT > 0 ? LT : d.L;
     const int K = d.K;
     const uint32_t U = LT > 0 ? (4 * LT - 1 + 31) / 32 * 32 : d.crt_u;
     const int nch = (K + 1 + static_cast<int>(kChunk) - 1) / static_cast<int>(kChunk);   // K + 1 rows
     const uint32_t tiles = (n_end - n_begin + kCrtTile - 1) / kCrtTile;
+    const uint32_t ys_n = lay.ystages;
     const uint64_t lim = d.wait_ns;
 
     if (threadIdx.x == 0) {
+        tc::mbar_init(sm.b_full, 1);
         for (int i = 0; i < 2; ++i) {
-            tc::mbar_init(&sm.b_full[i], 1);
-            tc::mbar_init(&sm.b_empty[i], 1);
             tc::mbar_init(&sm.a_full[i], kCrtTile);
             tc::mbar_init(&sm.a_empty[i], 1);
             tc::mbar_init(&sm.d_full[i], 1);
             tc::mbar_init(&sm.d_empty[i], kCrtTile);
             tc::mbar_init(&sm.m_full[i], kCrtTile);
             tc::mbar_init(&sm.m_empty[i], kCrtTile);
-            tc::mbar_init(&sm.o_sync[i], kCrtTile);
         }
-        for (int i = 0; i < kYStages; ++i) {
+        for (uint32_t i = 0; i < ys_n; ++i) {
             tc::mbar_init(&sm.y_full[i], 1);
             tc::mbar_init(&sm.y_empty[i], kCrtTile);
         }
         *sm.abort = 0;
         tc::fence_mbar_init();
+        // The constant image is read-only plan data: it loads under the
+        // preceding kernel's tail.  (Test hook: with kFaultCrt it is never
+        // requested, so the MMA issuer's wait for it runs out.)
+        if (!(d.fault & kFaultCrt)) {
+            tc::mbar_arrive_expect_tx(sm.b_full, lay.b_bytes);
+            const uint32_t chunk_bytes = U * 128;
+            for (uint32_t off = 0; off < lay.b_bytes; off += chunk_bytes) {
+                const uint32_t n = lay.b_bytes - off < chunk_bytes ? lay.b_bytes - off : chunk_bytes;
+                tc::bulk_g2s(sm.b + off, d.crt_img_v + off, n, sm.b_full);
+            }
+        }
     }
     if (warp == kYWarp && lane == 0) tc::prefetch_tmap(&tmY);
     if (warp == 0) tc::tmem_alloc(sm.tmem_base, 512);
@@ -181,45 +197,22 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc::tc_fence_after();
     const uint32_t tmem = *sm.tmem_base;
 
-    if (warp == kBWarp) {
-        // ---- constant chunks (read-only plan data: no wait for the
-        // preceding kernel) ----
-        if (lane == 0) {
-            const uint32_t bbytes = U * 128;
-            uint32_t par[2] = {0, 0};
-            bool armed[2] = {false, false};
-            uint32_t g = 0;
-            bool ok = true;
-            for (uint32_t t = blockIdx.x; ok && t < tiles; t += gridDim.x) {
-                for (int c = 0; c < nch; ++c, ++g) {
-                    const int s = g & 1;
-                    if (g >= 2 && !(ok = tc::wait_or_abort(&sm.b_empty[s], ((g - 2) >> 1) & 1, sm.abort, lim))) break;
-                    if (g == 0 && (d.fault & kFaultCrt)) continue;   // test hook: this phase never completes
-                    tc::mbar_arrive_expect_tx(&sm.b_full[s], bbytes);
-                    tc::bulk_g2s(sm.b + s * kBSlot, d.crt_img_v + static_cast<size_t>(c) * bbytes, bbytes,
-                                 &sm.b_full[s]);
-                    par[s] = (g >> 1) & 1;
-                    armed[s] = true;
-                }
-            }
-            // Copies still in flight must land before the CTA may exit.
-            for (int s = 0; s < 2; ++s) {
-                if (armed[s]) tc::wait_parity(&sm.b_full[s], par[s], lim);
-            }
-        }
+    if (warp == 0) {
+        // The constant image must land before the CTA may exit (after an abort too).
+        if (lane == 0 && !(d.fault & kFaultCrt)) tc::wait_parity(sm.b_full, 0, lim);
         __syncwarp();
     } else if (warp == kYWarp) {
         // ---- y boxes through the TMA ring ----
         if (lane == 0) {
             pdl_wait();   // y is the preceding kernel's output
-            uint32_t par[kYStages] = {};
-            bool armed[kYStages] = {};
+            uint32_t par[kMaxYStages] = {};
+            bool armed[kMaxYStages] = {};
             uint32_t g = 0;
             bool ok = true;
             for (uint32_t t = blockIdx.x; ok && t < tiles; t += gridDim.x) {
                 const int x = static_cast<int>(n_begin + t * kCrtTile);
                 for (int c = 0; c < nch; ++c, ++g) {
-                    const uint32_t s = g % kYStages, u = g / kYStages;
+                    const uint32_t s = g % ys_n, u = g / ys_n;
                     if (u >= 1 && !(ok = tc::wait_or_abort(&sm.y_empty[s], (u - 1) & 1, sm.abort, lim))) break;
                     tc::mbar_arrive_expect_tx(&sm.y_full[s], kYSlot);
                     tc::tma_load_2d(sm.y + s * (kYSlot / 4), &tmY, x, c * static_cast<int>(kChunk), &sm.y_full[s]);
@@ -227,7 +220,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                     armed[s] = true;
                 }
             }
-            for (int s = 0; s < kYStages; ++s) {
+            for (uint32_t s = 0; s < ys_n; ++s) {
                 if (armed[s]) tc::wait_parity(&sm.y_full[s], par[s], lim);
             }
         }
@@ -239,18 +232,17 @@ __global__ void __launch_bounds__(kThreads, 1)
             uint32_t g = 0, i = 0;
             uint64_t* last_bar = nullptr;
             uint32_t last_par = 0;
-            bool ok = true;
+            bool ok = tc::wait_or_abort(sm.b_full, 0, sm.abort, lim);
             for (uint32_t t = blockIdx.x; ok && t < tiles; t += gridDim.x, ++i) {
                 const uint32_t buf = i & 1, use = i >> 1;
                 if (use >= 1 && !(ok = tc::wait_or_abort(&sm.d_empty[buf], (use - 1) & 1, sm.abort, lim))) break;
                 for (int c = 0; c < nch; ++c, ++g) {
                     const int s = g & 1;
                     const uint32_t ph = (g >> 1) & 1;
-                    ok = tc::wait_or_abort(&sm.b_full[s], ph, sm.abort, lim) &&
-                         tc::wait_or_abort(&sm.a_full[s], ph, sm.abort, lim);
+                    ok = tc::wait_or_abort(&sm.a_full[s], ph, sm.abort, lim);
                     if (!ok) break;
                     tc::tc_fence_after();
-                    const uint32_t a0 = tc::smem_addr(sm.a + s * kASlot), b0 = tc::smem_addr(sm.b + s * kBSlot);
+                    const uint32_t a0 = tc::smem_addr(sm.a + s * kASlot), b0 = tc::smem_addr(sm.b + c * U * 128);
                     // K steps of 8 rows; the last chunk stops after row K.
                     const int rows_c = min(static_cast<int>(kChunk), K + 1 - c * static_cast<int>(kChunk));
                     const uint32_t ksteps = static_cast<uint32_t>(rows_c + 7) / 8;
@@ -260,8 +252,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                         tc::mma_u8(tmem + buf * 256, ad, bd, idesc, c > 0 || kk > 0);
                     }
                     tc::mma_commit(&sm.a_empty[s]);
-                    tc::mma_commit(&sm.b_empty[s]);
-                    last_bar = &sm.b_empty[s];
+                    last_bar = &sm.a_empty[s];
                     last_par = ph;
                 }
                 if (!ok) break;
@@ -285,7 +276,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int c = 0; c < kMaxChunks; ++c) {
                 if (c >= nch) break;
                 uint32_t yv[kChunk];
-                const uint32_t ys = g % kYStages, yu = g / kYStages;
+                const uint32_t ys = g % ys_n, yu = g / ys_n;
                 ok = tc::wait_or_abort(&sm.y_full[ys], yu & 1, sm.abort, lim);
                 ok = __all_sync(0xffffffffu, ok);
                 if (!ok) break;
@@ -351,11 +342,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t npieces = U / 16;
         const int n = L + 2, drop = top_drop(L);
         const uint32_t top_piece = static_cast<uint32_t>(4 * drop) / 16;
-        const bool svec = (L & 3) == 0;                                             // 16-byte rows in outs
-        const bool gvec = svec && (reinterpret_cast<uintptr_t>(C) & 15) == 0;      // 16-byte global stores
-        const int ostride = LT > 0 ? out_stride(LT) : out_stride(L);
-        uint32_t* const obase = sm.outs + grp * kCrtTile * ostride;
-        uint32_t* srow = obase + row * ostride;
+        const bool gvec = (L & 3) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;   // 16-byte row stores
         constexpr int kXL = LT > 0 ? LT + 2 : kX;        // limbs handled
         constexpr int kPieces = (kXL + 3) / 4;
         uint32_t k = 0;   // this group's tiles so far
@@ -363,6 +350,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t n0 = n_begin + t * kCrtTile;
             const uint32_t rows_t = min(kCrtTile, n_end - n0);
             const bool live = row < rows_t;
+            uint32_t* crow = C + static_cast<size_t>(n0 + (live ? row : 0)) * L;
             bool ok = tc::wait_or_abort(&sm.m_full[grp], k & 1, sm.abort, lim);
             ok = __all_sync(0xffffffffu, ok);
             if (!ok) break;
@@ -428,11 +416,11 @@ __global__ void __launch_bounds__(kThreads, 1)
                         b0 = static_cast<uint32_t>(dy >> 63);
                         b1 = static_cast<uint32_t>((static_cast<uint64_t>(yk) - qk - b1) >> 63);
                         o[ii] = yk;
-                        if (kl < L) {
-                            if (svec) {
-                                if (ii == 3) *reinterpret_cast<uint4*>(srow + kl - 3) = make_uint4(o[0], o[1], o[2], o[3]);
+                        if (kl < L && live) {
+                            if (gvec) {
+                                if (ii == 3) *reinterpret_cast<uint4*>(crow + kl - 3) = make_uint4(o[0], o[1], o[2], o[3]);
                             } else {
-                                srow[kl] = yk;
+                                crow[kl] = yk;
                             }
                         }
                     }
@@ -446,46 +434,18 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (live && (b0 || !b1)) {
                 uint32_t cb = 0;
                 for (int kk = 0; kk < L; ++kk) {
-                    const uint32_t x = srow[kk], qk = cc.q[kk];
+                    const uint32_t x = crow[kk], qk = cc.q[kk];
                     if (b0) {
                         const uint64_t sum = static_cast<uint64_t>(x) + qk + cb;
-                        srow[kk] = static_cast<uint32_t>(sum);
+                        crow[kk] = static_cast<uint32_t>(sum);
                         cb = static_cast<uint32_t>(sum >> 32);
                     } else {
                         const uint64_t dd = static_cast<uint64_t>(x) - qk - cb;
-                        srow[kk] = static_cast<uint32_t>(dd);
+                        crow[kk] = static_cast<uint32_t>(dd);
                         cb = static_cast<uint32_t>(dd >> 63);
                     }
                 }
             }
-            // The tile's rows are one contiguous run of c: copy it out with
-            // coalesced stores once every row of the group is staged.
-            tc::mbar_arrive(&sm.o_sync[grp]);
-            ok = tc::wait_or_abort(&sm.o_sync[grp], 0, sm.abort, lim);
-            ok = __all_sync(0xffffffffu, ok);
-            if (!ok) break;
-            {
-                uint32_t* gbase = C + static_cast<size_t>(n0) * L;
-                if (gvec) {
-                    const int q4 = L / 4, n4 = static_cast<int>(rows_t) * q4;
-                    for (int i4 = static_cast<int>(row); i4 < n4; i4 += kCrtTile) {
-                        const int r = i4 / q4, c4 = i4 - r * q4;
-                        *reinterpret_cast<uint4*>(gbase + 4 * i4) =
-                            *reinterpret_cast<const uint4*>(obase + r * ostride + 4 * c4);
-                    }
-                } else {
-                    const int nw = static_cast<int>(rows_t) * L;
-                    for (int i = static_cast<int>(row); i < nw; i += kCrtTile) {
-                        const int r = i / L;
-                        gbase[i] = obase[r * ostride + (i - r * L)];
-                    }
-                }
-            }
-            // The staged rows may be overwritten once every thread has copied.
-            tc::mbar_arrive(&sm.o_sync[grp]);
-            ok = tc::wait_or_abort(&sm.o_sync[grp], 1, sm.abort, lim);
-            ok = __all_sync(0xffffffffu, ok);
-            if (!ok) break;
         }
     }
 
@@ -501,7 +461,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 template <int LT>
 void set_attr() {
     check(cudaFuncSetAttribute(k_crt_pipe<LT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(kSmemBytes)),
+                               static_cast<int>(kSmemLimit)),
           "crt_pipe smem");
 }
 
@@ -520,9 +480,10 @@ CrtConsts make_crt_consts(const HostPlan& pl, const uint32_t* top) {
 
 bool crt_pipe_supported(const DevPoint& d, const uint32_t* Y, uint32_t n_begin, uint32_t n_end) {
     // TMA boxes of y: 16-byte aligned base, row pitch (N words) and column
-    // coordinates (n_begin) a multiple of 4 words.
+    // coordinates (n_begin) a multiple of 4 words; the constants resident.
     return d.L >= 2 && d.crt_u <= 256 && d.K + 1 <= kMaxK && d.crt_img_v && (d.N & 3) == 0 && d.N >= kCrtTile &&
-           (n_begin & 3) == 0 && n_end <= d.N && (reinterpret_cast<uintptr_t>(Y) & 15) == 0;
+           (n_begin & 3) == 0 && n_end <= d.N && (reinterpret_cast<uintptr_t>(Y) & 15) == 0 &&
+           make_layout(d.K, d.crt_u).bytes() <= kSmemLimit;
 }
 
 void crt_pipe_init_attributes() {
@@ -538,15 +499,17 @@ void launch_crt_pipe(const DevPoint& d, const CrtConsts& cc, const uint32_t* Y, 
     if (n_end <= n_begin) return;
     const uint32_t tiles = (n_end - n_begin + kCrtTile - 1) / kCrtTile;
     const uint32_t grid = tiles < static_cast<uint32_t>(sms) ? tiles : static_cast<uint32_t>(sms);
+    const Layout lay = make_layout(d.K, d.crt_u);
     // y: K rows of N words, boxes of 32 primes x 128 coefficients.
     const CUtensorMap tm = make_tmap_u32(Y, static_cast<uint64_t>(d.K), d.N, d.N, kChunk, kCrtTile, TmaSwizzle::kNone);
+    const size_t smem = lay.bytes();
     cudaError_t e = cudaSuccess;
     switch (d.L) {
-        case 64: e = launch_pdl(k_crt_pipe<64>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, tm, c, n_begin, n_end); break;
-        case 55: e = launch_pdl(k_crt_pipe<55>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, tm, c, n_begin, n_end); break;
-        case 28: e = launch_pdl(k_crt_pipe<28>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, tm, c, n_begin, n_end); break;
-        case 8: e = launch_pdl(k_crt_pipe<8>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, tm, c, n_begin, n_end); break;
-        default: e = launch_pdl(k_crt_pipe<0>, dim3(grid), dim3(kThreads), kSmemBytes, st, d, cc, tm, c, n_begin, n_end); break;
+        case 64: e = launch_pdl(k_crt_pipe<64>, dim3(grid), dim3(kThreads), smem, st, d, cc, tm, c, n_begin, n_end, lay); break;
+        case 55: e = launch_pdl(k_crt_pipe<55>, dim3(grid), dim3(kThreads), smem, st, d, cc, tm, c, n_begin, n_end, lay); break;
+        case 28: e = launch_pdl(k_crt_pipe<28>, dim3(grid), dim3(kThreads), smem, st, d, cc, tm, c, n_begin, n_end, lay); break;
+        case 8: e = launch_pdl(k_crt_pipe<8>, dim3(grid), dim3(kThreads), smem, st, d, cc, tm, c, n_begin, n_end, lay); break;
+        default: e = launch_pdl(k_crt_pipe<0>, dim3(grid), dim3(kThreads), smem, st, d, cc, tm, c, n_begin, n_end, lay); break;
     }
     check(e, "crt launch");
 }

@@ -30,6 +30,8 @@
 #include "tmap.h"
 
 #include <algorithm>
+#include <cstdlib>
+#include <cstring>
 #include <type_traits>
 
 namespace fpm {
@@ -238,8 +240,12 @@ constexpr uint32_t kColTmaBox = 2048 * sizeof(uint32_t);                 // one 
 constexpr uint32_t kColTmaTw = 64 * sizeof(uint2);                       // R = 64 twiddles
 constexpr uint32_t kColFwdStage = 17 * 1024;                             // A, B, twiddles (1024-aligned)
 constexpr uint32_t kColInvStage = 9 * 1024;                              // A, twiddles
-constexpr size_t kColFwdTmaSmem = 2 * size_t(kColFwdStage) + 16;
-constexpr size_t kColInvTmaSmem = 2 * size_t(kColInvStage) + 16;
+// ST = 2: persistent, two buffers (next tile in flight); ST = 1: one tile
+// per CTA, one buffer, eight CTAs per SM (other CTAs' work covers a CTA's wait).
+template <int ST>
+constexpr size_t col_fwd_tma_smem() { return ST * size_t(kColFwdStage) + 16; }
+template <int ST>
+constexpr size_t col_inv_tma_smem() { return ST * size_t(kColInvStage) + 16; }
 
 template <int LOGS, bool FWD>
 __device__ __forceinline__ void col_tma_issue(const DevPoint& d, const CUtensorMap* tmA, const CUtensorMap* tmB,
@@ -253,8 +259,8 @@ __device__ __forceinline__ void col_tma_issue(const DevPoint& d, const CUtensorM
     tc::bulk_g2s(stage + (FWD ? 2 : 1) * kColTmaBox, tw, kColTmaTw, bar);
 }
 
-template <int LOGS, bool LAZY>
-__global__ void __launch_bounds__(256, 6)
+template <int LOGS, bool LAZY, int ST>
+__global__ void __launch_bounds__(256, ST == 1 ? 8 : 6)
     k_ntt_col_fwd_tma(DevPoint d, const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     constexpr int LOGR = 6, XS = 5, RB = 3, E = 8;
@@ -262,7 +268,7 @@ __global__ void __launch_bounds__(256, 6)
     static_assert(RP<LOGR, XS, SWZ, RB>::all_conflict_free(), "column rounds must be free of bank conflicts");
     constexpr int last = RP<LOGR, XS, SWZ, RB>::kCount - 1;
     constexpr uint32_t per = (1u << LOGS) / 32;
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + 2 * kColFwdStage);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + ST * kColFwdStage);
     const uint32_t tiles = per * static_cast<uint32_t>(d.K);
     if (threadIdx.x == 0) {
         tc::mbar_init(&full[0], 1);
@@ -277,13 +283,14 @@ __global__ void __launch_bounds__(256, 6)
     if (threadIdx.x == 0 && blockIdx.x < tiles) col_tma_issue<LOGS, true>(d, &tmA, &tmB, smem_raw, &full[0], blockIdx.x);
     uint32_t i = 0;
     for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++i) {
-        const int s = i & 1;
+        const int s = ST == 1 ? 0 : (i & 1);
         uint8_t* stage = smem_raw + s * kColFwdStage;
         uint32_t* const tiles2[2] = {reinterpret_cast<uint32_t*>(stage), reinterpret_cast<uint32_t*>(stage + kColTmaBox)};
         const SharedTable table{reinterpret_cast<const uint2*>(stage + 2 * kColTmaBox)};
         const uint32_t j = t / per;
         const uint32_t p = d.pc[j].p;
-        if (!tc::wait_parity(&full[s], (i >> 1) & 1, d.wait_ns) && threadIdx.x == 0) atomicOr(d.err, 4u);
+        if (!tc::wait_parity(&full[s], (ST == 1 ? i : i >> 1) & 1, d.wait_ns) && threadIdx.x == 0)
+            atomicOr(d.err, 4u);
         {
             const uint32_t base = round_base<LOGR, XS, SWZ, RB, 0>(threadIdx.x);
             uint32_t v[2][E];
@@ -296,7 +303,7 @@ __global__ void __launch_bounds__(256, 6)
         }
         // The next tile's loads, into the other buffer once the stores of the
         // tile that used it have read it.
-        if (threadIdx.x == 0 && t + gridDim.x < tiles) {
+        if (ST == 2 && threadIdx.x == 0 && t + gridDim.x < tiles) {
             tc::bulk_wait_read();
             col_tma_issue<LOGS, true>(d, &tmA, &tmB, smem_raw + (s ^ 1) * kColFwdStage, &full[s ^ 1], t + gridDim.x);
         }
@@ -322,7 +329,7 @@ __global__ void __launch_bounds__(256, 6)
     if (threadIdx.x == 0) tc::bulk_wait_all();
 }
 
-template <int LOGS, bool LAZY>
+template <int LOGS, bool LAZY, int ST>
 __global__ void __launch_bounds__(256, 8) k_ntt_col_inv_tma(DevPoint d, const __grid_constant__ CUtensorMap tmA) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     constexpr int LOGR = 6, XS = 5, RB = 3, E = 8;
@@ -330,7 +337,7 @@ __global__ void __launch_bounds__(256, 8) k_ntt_col_inv_tma(DevPoint d, const __
     static_assert(RP<LOGR, XS, SWZ, RB>::all_conflict_free(), "column rounds must be free of bank conflicts");
     constexpr int last = RP<LOGR, XS, SWZ, RB>::kCount - 1;
     constexpr uint32_t per = (1u << LOGS) / 32;
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + 2 * kColInvStage);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + ST * kColInvStage);
     const uint32_t tiles = per * static_cast<uint32_t>(d.K);
     if (threadIdx.x == 0) {
         tc::mbar_init(&full[0], 1);
@@ -344,13 +351,14 @@ __global__ void __launch_bounds__(256, 8) k_ntt_col_inv_tma(DevPoint d, const __
     if (threadIdx.x == 0 && blockIdx.x < tiles) col_tma_issue<LOGS, false>(d, &tmA, &tmA, smem_raw, &full[0], blockIdx.x);
     uint32_t i = 0;
     for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x, ++i) {
-        const int s = i & 1;
+        const int s = ST == 1 ? 0 : (i & 1);
         uint8_t* stage = smem_raw + s * kColInvStage;
         uint32_t* ta = reinterpret_cast<uint32_t*>(stage);
         const SharedTable table{reinterpret_cast<const uint2*>(stage + kColTmaBox)};
         const uint32_t j = t / per;
         const uint32_t p = d.pc[j].p;
-        if (!tc::wait_parity(&full[s], (i >> 1) & 1, d.wait_ns) && threadIdx.x == 0) atomicOr(d.err, 4u);
+        if (!tc::wait_parity(&full[s], (ST == 1 ? i : i >> 1) & 1, d.wait_ns) && threadIdx.x == 0)
+            atomicOr(d.err, 4u);
         {
             const uint32_t base = round_base<LOGR, XS, SWZ, RB, last>(threadIdx.x);
             uint32_t v[E];
@@ -359,7 +367,7 @@ __global__ void __launch_bounds__(256, 8) k_ntt_col_inv_tma(DevPoint d, const __
             store_round<LOGR, XS, SWZ, RB, last>(ta, v, base);
             __syncthreads();
         }
-        if (threadIdx.x == 0 && t + gridDim.x < tiles) {
+        if (ST == 2 && threadIdx.x == 0 && t + gridDim.x < tiles) {
             tc::bulk_wait_read();
             col_tma_issue<LOGS, false>(d, &tmA, &tmA, smem_raw + (s ^ 1) * kColInvStage, &full[s ^ 1], t + gridDim.x);
         }
@@ -921,11 +929,17 @@ void group_pass(const GroupTable* t, int pass, uint32_t logR, uint32_t logS, uin
 
 template <int LOGS, bool LAZY>
 void col_tma_attrs() {
-    check(cudaFuncSetAttribute(k_ntt_col_fwd_tma<LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(kColFwdTmaSmem)),
+    check(cudaFuncSetAttribute(k_ntt_col_fwd_tma<LOGS, LAZY, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(col_fwd_tma_smem<1>())),
           "col smem");
-    check(cudaFuncSetAttribute(k_ntt_col_inv_tma<LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               static_cast<int>(kColInvTmaSmem)),
+    check(cudaFuncSetAttribute(k_ntt_col_inv_tma<LOGS, LAZY, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(col_inv_tma_smem<1>())),
+          "col smem");
+    check(cudaFuncSetAttribute(k_ntt_col_fwd_tma<LOGS, LAZY, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(col_fwd_tma_smem<2>())),
+          "col smem");
+    check(cudaFuncSetAttribute(k_ntt_col_inv_tma<LOGS, LAZY, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               static_cast<int>(col_inv_tma_smem<2>())),
           "col smem");
 }
 
@@ -971,16 +985,37 @@ CUtensorMap col_tmap(const DevPoint& d, const uint32_t* X) {
     return make_tmap_u32(X, static_cast<uint64_t>(d.K) << 6, d.N >> 6, d.N >> 6, 64, 32, TmaSwizzle::k128B);
 }
 
+// Column-pass variant: FPM_COL_PASS = tma1 (TMA, one tile per CTA; the
+// default), tma2 (TMA, persistent, two buffers) or plain (per-thread loads
+// and stores), read once.
+int col_pass_variant() {
+    static const int v = [] {
+        const char* e = std::getenv("FPM_COL_PASS");
+        if (!e) return 1;
+        if (!std::strcmp(e, "plain")) return 0;
+        if (!std::strcmp(e, "tma2")) return 2;
+        return 1;
+    }();
+    return v;
+}
+
 template <bool LAZY>
 void launch_col_fwd_t(const DevPoint& d, uint32_t* A, uint32_t* B, cudaStream_t st) {
-    if (col_tma_ok(d, A, B)) {
+    const int var = col_pass_variant();
+    if (var && col_tma_ok(d, A, B)) {
         with_log(d.logS, [&](auto s) {
             constexpr int LS = decltype(s)::value;
             const uint32_t tiles = ((1u << LS) / 32) * static_cast<uint32_t>(d.K);
-            const uint32_t grid = std::min<uint32_t>(tiles, 6u * static_cast<uint32_t>(device_sms()));
-            check(launch_pdl(k_ntt_col_fwd_tma<LS, LAZY>, dim3(grid), dim3(256), kColFwdTmaSmem, st, d, col_tmap(d, A),
-                             col_tmap(d, B)),
-                  "col_fwd launch");
+            if (var == 2) {
+                const uint32_t grid = std::min<uint32_t>(tiles, 6u * static_cast<uint32_t>(device_sms()));
+                check(launch_pdl(k_ntt_col_fwd_tma<LS, LAZY, 2>, dim3(grid), dim3(256), col_fwd_tma_smem<2>(), st, d,
+                                 col_tmap(d, A), col_tmap(d, B)),
+                      "col_fwd launch");
+            } else {
+                check(launch_pdl(k_ntt_col_fwd_tma<LS, LAZY, 1>, dim3(tiles), dim3(256), col_fwd_tma_smem<1>(), st, d,
+                                 col_tmap(d, A), col_tmap(d, B)),
+                      "col_fwd launch");
+            }
         });
         return;
     }
@@ -995,14 +1030,21 @@ void launch_col_fwd_t(const DevPoint& d, uint32_t* A, uint32_t* B, cudaStream_t 
 
 template <bool LAZY>
 void launch_col_inv_t(const DevPoint& d, uint32_t* A, cudaStream_t st) {
-    if (col_tma_ok(d, A, A)) {
+    const int var = col_pass_variant();
+    if (var && col_tma_ok(d, A, A)) {
         with_log(d.logS, [&](auto s) {
             constexpr int LS = decltype(s)::value;
             const uint32_t tiles = ((1u << LS) / 32) * static_cast<uint32_t>(d.K);
-            const uint32_t grid = std::min<uint32_t>(tiles, 8u * static_cast<uint32_t>(device_sms()));
-            check(launch_pdl(k_ntt_col_inv_tma<LS, LAZY>, dim3(grid), dim3(256), kColInvTmaSmem, st, d,
-                             col_tmap(d, A)),
-                  "col_inv launch");
+            if (var == 2) {
+                const uint32_t grid = std::min<uint32_t>(tiles, 8u * static_cast<uint32_t>(device_sms()));
+                check(launch_pdl(k_ntt_col_inv_tma<LS, LAZY, 2>, dim3(grid), dim3(256), col_inv_tma_smem<2>(), st, d,
+                                 col_tmap(d, A)),
+                      "col_inv launch");
+            } else {
+                check(launch_pdl(k_ntt_col_inv_tma<LS, LAZY, 1>, dim3(tiles), dim3(256), col_inv_tma_smem<1>(), st, d,
+                                 col_tmap(d, A)),
+                      "col_inv launch");
+            }
         });
         return;
     }
