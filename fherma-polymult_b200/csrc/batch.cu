@@ -217,8 +217,11 @@ int enqueue_grouped(const std::vector<GroupedProduct>& prods_, const BatchSchedu
         for (int pass : {int(kPassColFwd), int(kPassRow), int(kPassColInv)}) {
             uint32_t grid = 0;
             if (sched_.grid > 0) {
+                // (Sub-batches of the host path may have a smaller largest row.)
+                const auto it = env.occupancy->find(occupancy_key(pass, 63, max_log_s, lazy));
+                const int occ = it != env.occupancy->end() ? it->second : ntt_mixed_occupancy(pass, lazy, max_log_s);
                 grid = static_cast<uint32_t>(sched_.grid) * static_cast<uint32_t>(env.sms) *
-                       static_cast<uint32_t>(std::max(1, env.occupancy->at(occupancy_key(pass, 63, max_log_s, lazy))));
+                       static_cast<uint32_t>(std::max(1, occ));
             }
             fill.reset();
             auto flush = [&] {

@@ -58,7 +58,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 
 // As mbar_try_wait, but the thread may sleep in hardware (up to about
 // kSuspendNs) until the phase completes, instead of spinning.
-constexpr uint32_t kSuspendNs = 500000;
+#ifndef FPM_SUSPEND_NS
+#define FPM_SUSPEND_NS 500000
+#endif
+constexpr uint32_t kSuspendNs = FPM_SUSPEND_NS;
 
 __device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity) {
     uint32_t ok;
@@ -125,6 +128,14 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, const void*
     asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
                      reinterpret_cast<uint64_t>(map)),
                  "r"(x), "r"(y), "r"(smem_addr(src))
+                 : "memory");
+}
+
+// Shared -> global bulk copy (both addresses 16-byte aligned, bytes a multiple
+// of 16), tracked like the tensor stores.
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)),
+                 "r"(bytes)
                  : "memory");
 }
 
