@@ -126,6 +126,18 @@ FPM_HD void gs_butterfly(uint32_t& x, uint32_t& y, uint2 w, uint32_t p) {
     y = shoup(sub_mod(u, v, p), w.x, w.y, p);
 }
 
+// Tensor-core operand images in the UMMA K-major 128-byte-swizzle layout: a
+// row's K bytes split in 128-byte halves, each half a block of rows x 128
+// bytes; row r of a half at r * 128, its 16-byte chunk c at (c ^ (r % 8)) * 16
+// (the swizzle the tensor cores undo on the fly; blocks 1024-byte aligned).
+FPM_HD size_t sw128_offset(uint32_t row, uint32_t k, uint32_t rows) {
+    const uint32_t half = k >> 7, c = (k >> 4) & 7u;
+    return static_cast<size_t>(half) * rows * 128 + static_cast<size_t>(row) * 128 + (((c ^ (row & 7u)) << 4) | (k & 15u));
+}
+FPM_HD size_t sw128_bytes(uint32_t rows, uint32_t kbytes) {
+    return static_cast<size_t>(rows) * 128 * ((kbytes + 127) / 128);
+}
+
 FPM_HD uint32_t bitrev(uint32_t x, uint32_t bits) {
     if (bits == 0) return 0;
 #if defined(__CUDA_ARCH__)

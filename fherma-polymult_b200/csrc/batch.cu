@@ -124,7 +124,7 @@ int enqueue_grouped(const std::vector<GroupedProduct>& prods_, const BatchSchedu
                 ++launches_;
                 continue;
             }
-            if (piped(p) && p.e->crt_consts() && crt_pipe_supported(p.d, p.A, 0, p.d.N)) {
+            if (piped(p) && p.e->crt_consts() && crt_pipe_supported(p.d, *p.e->crt_consts(), p.A, 0, p.d.N)) {
                 launch_crt_pipe(p.d, *p.e->crt_consts(), p.A, p.c, 0, p.d.N, p.e->sms(), s);
                 ++launches_;
                 continue;

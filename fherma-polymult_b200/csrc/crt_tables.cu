@@ -4,7 +4,8 @@
 //   negvP_v = (q - v P mod q) mod q, v = 0 .. K        ((K + 1) x L)
 //   the tensor-core CRT images (plan.h): crt_img holds M_j's low L - 1 limbs
 //   byte-shifted into GEMM columns, crt_img_v the same with a row K for
-//   negvP_1 = -P mod q.
+//   negvP_1 = -P mod q (in the pipelined CRT's layout: every chunk but the
+//   last 128-byte swizzled).
 //
 // Reference counterpart: rns_plan.h:224-247, where make_plan builds M_j and
 // negvP on the host with an O(K^2 L) loop (one product of K - 1 primes mod q
@@ -66,21 +67,19 @@ __global__ void k_crt_negvp(const uint32_t* Pq, int K, const uint32_t* q, int L,
 
 // Image row j (constant m, L limbs) into GEMM column 4 (j % 32) + s of chunk
 // j / 32, byte position u: byte (u - s) of m's low L - 1 limbs.  One thread
-// per (row, u); the image was zeroed.
+// per (row, u); the image was zeroed.  Layout (crt_image_at): plain core
+// matrices, or with swz every chunk but the last 128-byte swizzled.
 __global__ void k_crt_image(const uint32_t* M, const uint32_t* negvP, int K, int L, uint32_t crt_u, int rows,
-                            uint8_t* img) {
+                            bool swz, uint8_t* img) {
     const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t j = idx / crt_u, u = idx - j * crt_u;
     if (j >= static_cast<uint32_t>(rows)) return;
     const uint32_t* m = j < static_cast<uint32_t>(K) ? M + static_cast<size_t>(j) * L : negvP + L;
-    const size_t cchunk = static_cast<size_t>(crt_u) * 128;
     const uint32_t low_bytes = 4 * static_cast<uint32_t>(L - 1);
     for (uint32_t s = 0; s < 4 && s <= u; ++s) {
         const uint32_t byte = u - s;
         if (byte >= low_bytes) continue;
-        const uint32_t kbyte = 4 * (j % 32) + s;
-        const size_t at = static_cast<size_t>(j / 32) * cchunk + (kbyte / 16) * (crt_u * 16) + u * 16 + (kbyte % 16);
-        img[at] = static_cast<uint8_t>(m[byte / 4] >> (8 * (byte % 4)));
+        img[crt_image_at(j, s, u, crt_u, rows, swz)] = static_cast<uint8_t>(m[byte / 4] >> (8 * (byte % 4)));
     }
 }
 
@@ -103,7 +102,7 @@ void build_crt_tables(const HostPlan& pl, const PrimeConsts* pc, const uint32_t*
     for (int i = 0; i < 2; ++i) {
         check(cudaMemsetAsync(out[i], 0, crt_image_bytes(pl, rows[i]), st), "crt image clear");
         const uint32_t threads = static_cast<uint32_t>(rows[i]) * pl.crt_u;
-        k_crt_image<<<(threads + 255) / 256, 256, 0, st>>>(M, negvP, K, L, pl.crt_u, rows[i], out[i]);
+        k_crt_image<<<(threads + 255) / 256, 256, 0, st>>>(M, negvP, K, L, pl.crt_u, rows[i], i == 1, out[i]);
         check(cudaGetLastError(), "crt image launch");
     }
 }

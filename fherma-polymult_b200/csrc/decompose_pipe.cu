@@ -13,7 +13,8 @@
 //     widest shape (N = 256 columns per chunk): D goes to one of two
 //     256-column TMEM buffers;
 //   * warps 1-4 copy each tile's limbs into a two-slot ring in the MMA's
-//     K-major layout with asynchronous copies (cp.async), one tile in flight
+//     128-byte-swizzled K-major layout (the layout the tensor cores read at
+//     full rate) with asynchronous copies (cp.async), one tile in flight
 //     while the previous one lands and is multiplied: a warp moves 8 rows x 4
 //     sixteen-byte groups at a time, so the global loads are 64-byte runs and
 //     the eight lanes of each shared-store phase hit eight different bank
@@ -41,11 +42,13 @@ constexpr int kEpiWarp0 = 5;                       // warps 5-20
 constexpr int kEpi = 512;
 constexpr uint32_t kRows = 128;
 constexpr uint32_t kCols = 256;                    // GEMM columns per full chunk (64 primes)
-constexpr uint32_t kALbo = kRows * 16;             // K stride of the operand tile (128-byte aligned)
 
-__host__ __device__ inline uint32_t a_bytes(uint32_t kb) { return (kb / 16) * kALbo; }
+// Operand tiles and the constant image in the 128-byte-swizzle layout
+// (sw128_offset): a tile is 128 rows, a constant chunk 256 columns (the last
+// nlast), each with kb K bytes.
+__host__ __device__ inline uint32_t a_bytes(uint32_t kb) { return static_cast<uint32_t>(sw128_bytes(kRows, kb)); }
 __host__ __device__ inline size_t b_bytes(uint32_t kb, int nch, uint32_t nlast) {
-    return (static_cast<size_t>(nch) - 1) * kCols * kb + static_cast<size_t>(nlast) * kb;
+    return (static_cast<size_t>(nch) - 1) * sw128_bytes(kCols, kb) + sw128_bytes(nlast, kb);
 }
 __host__ inline size_t smem_bytes(uint32_t kb, int nch, uint32_t nlast) {
     return b_bytes(kb, nch, nlast) + 2 * a_bytes(kb) + 128;
@@ -120,6 +123,12 @@ __global__ void __launch_bounds__(kThreads, 1)
                      int operand0, uint32_t n_begin, uint32_t n_end, uint32_t split) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     pdl_launch_dependents();
+    // The 128-byte swizzle is a function of the shared address: the
+    // operand atoms need a 1024-byte aligned base (error bit 4 otherwise).
+    if (tc::smem_addr(smem_raw) & 1023u) {
+        if (threadIdx.x == 0) atomicOr(d.err, 4u);
+        return;
+    }
     const uint32_t kb = d.dec_kb;
     const int nch = static_cast<int>(fc.chunks);
     const uint32_t nlast = fc.last_cols;
@@ -133,7 +142,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     const uint8_t* img = fc.img[operand];
     const uint32_t g0 = second ? split : 0, gs = second ? gridDim.x - split : split;
     const uint32_t tiles = (n_end - n_begin + kRows - 1) / kRows;
-    const uint32_t chunk_bytes = kCols * kb;
+    const uint32_t chunk_bytes = static_cast<uint32_t>(sw128_bytes(kCols, kb));
     const uint64_t lim = d.wait_ns;
 
     if (threadIdx.x == 0) {
@@ -192,8 +201,9 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint32_t cols = lastc ? nlast : kCols;
                     const uint32_t b0 = tc::smem_addr(sm.b + c * chunk_bytes);
                     for (uint32_t kk = 0; kk < kb / 32; ++kk) {
-                        const uint64_t ad = tc::smem_desc(a0 + kk * 2 * kALbo, kALbo, 128);
-                        const uint64_t bd = tc::smem_desc(b0 + kk * 2 * (cols * 16), cols * 16, 128);
+                        const uint32_t half = kk >> 2, step = (kk & 3) * 32;
+                        const uint64_t ad = tc::smem_desc_sw128(a0 + half * kRows * 128 + step);
+                        const uint64_t bd = tc::smem_desc_sw128(b0 + half * cols * 128 + step);
                         tc::mma_u8(tmem + buf * kCols, ad, bd, lastc ? idesc_last : idesc_full, kk > 0);
                     }
                     tc::mma_commit(&sm.d_full[buf]);
@@ -244,7 +254,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                     const uint32_t mm = 8 * (blk & 15) + r, gq = 4 * (blk >> 4) + gi;
                     if (gq < G) {
                         const bool have = mm < nk && gq < q4;
-                        cp_async16_zfill(at + gq * kALbo + mm * 16, have ? src4 + mm * q4 + gq : src4, have);
+                        cp_async16_zfill(at + sw128_offset(mm, 16 * gq, kRows), have ? src4 + mm * q4 + gq : src4,
+                                         have);
                     }
                 }
             } else {
@@ -253,8 +264,7 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (uint32_t blk = lw; blk < 16 * G; blk += kLoaders / 32) {
                     const uint32_t mm = 8 * (blk & 15) + r, l = 4 * (blk >> 4) + gi;
                     const bool have = mm < nk && l < static_cast<uint32_t>(L);
-                    cp_async4_zfill(at + (l >> 2) * kALbo + mm * 16 + (l & 3) * 4,
-                                    have ? src + mm * L + l : src, have);
+                    cp_async4_zfill(at + sw128_offset(mm, 4 * l, kRows), have ? src + mm * L + l : src, have);
                 }
             }
             cp_async_commit();

@@ -270,7 +270,7 @@ void Engine::launch_crt_any(const DevPoint& d, const uint32_t* d_y, uint32_t* d_
                             cudaStream_t st) {
     if (simt_ || !crt_uses_tc(plan_)) {
         launch_crt(d, d_y, d_c, n0, n1, st);
-    } else if (crt_consts_ && crt_pipe_supported(d, d_y, n0, n1)) {
+    } else if (crt_consts_ && crt_pipe_supported(d, *crt_consts_, d_y, n0, n1)) {
         launch_crt_pipe(d, *crt_consts_, d_y, d_c, n0, n1, sms_, st);
     } else {
         launch_crt_tc(d, d_y, d_c, n0, n1, st);

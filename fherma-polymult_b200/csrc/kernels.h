@@ -77,9 +77,11 @@ void launch_crt_tc(const DevPoint& d, const uint32_t* Y, uint32_t* c, uint32_t n
 // Needs L >= 2 and N, n_begin, n_end multiples of 4.  Its per-prime constants
 // travel as a kernel parameter.
 struct CrtConsts {
-    uint32_t r50[kMaxK];        // floor(2^50 / p_j), for the rounding sum
-    uint32_t mlo[kMaxK + 1];    // top limb of constant j (j = K: -P mod q), low 16 bits
-    uint32_t mhi[kMaxK + 1];    // and high 16 bits
+    float cf[kMaxK];            // 2^sh_j / p_j in single precision, for the rounding sum
+    uint32_t sh[kMaxK];         // sh_j: y_j >> sh_j < 2^23 and 2^(23 + sh_j) / p_j <= 2
+    float voff;                 // sum_j 2^23 cf_j: the offset the rounding sum removes
+    float est_err;              // a bound on the rounding sum's error (must stay below 1/4)
+    uint32_t top[kMaxK + 1];    // top limb of constant j (j = K: -P mod q)
     uint32_t q[kMaxL + 2];      // q, zero above L
 };
 // top: the K constants' top limbs M_j[L - 1], then (-P mod q)'s top limb.
@@ -92,7 +94,7 @@ CrtConsts make_crt_consts(const HostPlan& pl, const uint32_t* top);
 size_t crt_image_bytes(const HostPlan& pl, int rows);
 void build_crt_tables(const HostPlan& pl, const PrimeConsts* pc, const uint32_t* q, uint32_t* M, uint32_t* negvP,
                       uint32_t* Pq, uint8_t* img, uint8_t* img_v, cudaStream_t st);
-bool crt_pipe_supported(const DevPoint& d, const uint32_t* Y, uint32_t n_begin, uint32_t n_end);
+bool crt_pipe_supported(const DevPoint& d, const CrtConsts& cc, const uint32_t* Y, uint32_t n_begin, uint32_t n_end);
 void crt_pipe_init_attributes();
 void launch_crt_pipe(const DevPoint& d, const CrtConsts& cc, const uint32_t* Y, uint32_t* c, uint32_t n_begin,
                      uint32_t n_end, int sms, cudaStream_t st);

@@ -278,8 +278,8 @@ HostPlan make_plan_basis(uint32_t N, uint32_t W, int L, int qbits, int pmax_log2
     // the last chunk packed to its own width, a multiple of 16 columns.
     pl.dec_wchunks = static_cast<uint32_t>((K + 63) / 64);
     pl.dec_wlast = (4 * static_cast<uint32_t>(K - 64 * (static_cast<int>(pl.dec_wchunks) - 1)) + 15) / 16 * 16;
-    const size_t wchunk = static_cast<size_t>(256) * pl.dec_kb;
-    pl.dec_wimg_a.assign(wchunk * (pl.dec_wchunks - 1) + static_cast<size_t>(pl.dec_wlast) * pl.dec_kb, 0);
+    const size_t wchunk = sw128_bytes(256, pl.dec_kb);   // 128-byte-swizzle layout (sw128_offset)
+    pl.dec_wimg_a.assign(wchunk * (pl.dec_wchunks - 1) + sw128_bytes(pl.dec_wlast, pl.dec_kb), 0);
     pl.dec_wimg_b.assign(pl.dec_wimg_a.size(), 0);
     for (int j = 0; j < K; ++j) {
         const uint32_t p = pl.primes[j];
@@ -297,7 +297,7 @@ HostPlan make_plan_basis(uint32_t N, uint32_t W, int L, int qbits, int pmax_log2
                 pl.dec_img_b[at] = static_cast<uint8_t>(cb >> (8 * s));
                 const uint32_t wc = static_cast<uint32_t>(j / 64), wcol = 4 * (j % 64) + s;
                 const uint32_t wcols = wc + 1 < pl.dec_wchunks ? 256 : pl.dec_wlast;
-                const size_t wat = wc * wchunk + (k / 16) * (wcols * 16) + wcol * 16 + (k % 16);
+                const size_t wat = wc * wchunk + sw128_offset(wcol, k, wcols);
                 pl.dec_wimg_a[wat] = static_cast<uint8_t>(ca >> (8 * s));
                 pl.dec_wimg_b[wat] = static_cast<uint8_t>(cb >> (8 * s));
             }
@@ -355,26 +355,24 @@ void set_modulus(HostPlan& pl, const uint32_t* q) {
         const size_t cchunk = static_cast<size_t>(pl.crt_u) * 128;
         const uint32_t low_bytes = 4 * static_cast<uint32_t>(L - 1);
         // Row j of an image holds the byte shifts of constant j's low L - 1 limbs.
-        auto build = [&](std::vector<uint8_t>& img, int rows, auto&& limbs_of) {
+        auto build = [&](std::vector<uint8_t>& img, int rows, bool swz, auto&& limbs_of) {
             img.assign(cchunk * static_cast<size_t>((rows + 31) / 32), 0);
             for (int j = 0; j < rows; ++j) {
                 const uint32_t* m = limbs_of(j);
                 for (int s = 0; s < 4; ++s) {
-                    const uint32_t kbyte = 4 * (j % 32) + s;   // K index within the chunk
                     for (uint32_t u = s; u < pl.crt_u && u - s < low_bytes; ++u) {
                         const uint32_t byte = u - s;
-                        const size_t at = static_cast<size_t>(j / 32) * cchunk + (kbyte / 16) * (pl.crt_u * 16) +
-                                          u * 16 + (kbyte % 16);
-                        img[at] = static_cast<uint8_t>(m[byte / 4] >> (8 * (byte % 4)));
+                        img[crt_image_at(j, s, u, pl.crt_u, rows, swz)] =
+                            static_cast<uint8_t>(m[byte / 4] >> (8 * (byte % 4)));
                     }
                 }
             }
         };
         (void)chunks;
-        build(pl.crt_img, K, [&](int j) { return &pl.M[static_cast<size_t>(j) * L]; });
+        build(pl.crt_img, K, false, [&](int j) { return &pl.M[static_cast<size_t>(j) * L]; });
         // The same with one more row, -P mod q: its multiplier is v, so the
         // GEMM itself adds -v P (the pipelined CRT needs no negvP table).
-        build(pl.crt_img_v, K + 1, [&](int j) {
+        build(pl.crt_img_v, K + 1, true, [&](int j) {
             return j < K ? &pl.M[static_cast<size_t>(j) * L] : &pl.negvP[static_cast<size_t>(L)];
         });
         pl.negp_top = pl.negvP[static_cast<size_t>(L) + L - 1];

@@ -104,6 +104,19 @@ struct HostPlan {
     uint32_t negp_top = 0;
 };
 
+// Byte of a CRT image: row j (a constant; K-byte 4 (j % 32) + s of chunk
+// j / 32) at GEMM column u, for images of `rows` rows and crt_u columns.
+// Plain: the core-matrix layout [8 core columns][crt_u][16 bytes] per chunk;
+// swz: every chunk but the last in the 128-byte-swizzle layout (sw128_offset),
+// the last plain (the pipelined CRT keeps only its first K steps resident).
+FPM_HD size_t crt_image_at(uint32_t j, uint32_t s, uint32_t u, uint32_t crt_u, int rows, bool swz) {
+    const uint32_t kbyte = 4 * (j % 32) + s, chunk = j / 32;
+    const size_t base = static_cast<size_t>(chunk) * crt_u * 128;
+    const uint32_t last = static_cast<uint32_t>(rows - 1) / 32;
+    if (swz && chunk < last) return base + sw128_offset(u, kbyte, crt_u);
+    return base + (kbyte / 16) * (crt_u * 16) + u * 16 + (kbyte % 16);
+}
+
 // Which CRT kernel the point uses: the tensor-core one needs L >= 2.
 inline bool crt_uses_tc(const HostPlan& pl) { return pl.L >= 2; }
 

@@ -207,6 +207,16 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
            (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
+// The same for the 128-byte-swizzle K-major layout (sw128_offset): 8-row
+// groups 1024 bytes apart; the start address of a K step inside the 128-byte
+// swizzle span is the block's address plus the step's byte offset (the
+// swizzle applies to the final address bits, the blocks being 1024-byte
+// aligned).
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (1ull << 16) | (static_cast<uint64_t>(1024 >> 4) << 32) |
+           (1ull << 46) | (2ull << 61);
+}
+
 // Instruction descriptor for kind::i8: u8 x u8 -> s32, both operands K-major,
 // M = 128, N = n (multiple of 16, <= 256).
 __host__ __device__ constexpr uint32_t idesc_u8(uint32_t n) {
