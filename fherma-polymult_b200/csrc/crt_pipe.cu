@@ -469,15 +469,28 @@ __global__ void __launch_bounds__(kThreads, 1)
                  ldexp(static_cast<double>(meta.x), 32 * (L - 1 - drop)) +
                  ldexp(static_cast<double>(meta.y), 32 * (L - drop)) +
                  ldexp(static_cast<double>(meta.z), 32 * (L + 1 - drop));
-            const double f = floor(xd * d.q_top_inv);
+            const double fq = xd * d.q_top_inv;
+            const double f = floor(fq);
             const uint64_t e = f > 0 ? static_cast<uint64_t>(f) : 0;
             const uint32_t e_lo = static_cast<uint32_t>(e), e_hi = static_cast<uint32_t>(e >> 32);
-            // One pass from the bottom: X with carries, minus e q; the borrows
-            // of X - e q (b0) and of (X - e q) - q (b1).  TMEM pieces are
-            // double-buffered: piece pc + 1 loads while piece pc is used.
-            uint64_t carry = 0, c0 = 0;
-            uint32_t b0 = 0, b1 = 0;
-            uint32_t o[4];
+            // With the fraction of the estimate at least 2^-8 from an integer,
+            // e = floor(X / q) exactly and X - e q lies in [0, q); otherwise it
+            // lies in [-q, 2q) and the row is checked after the pass.
+            const double frac = fq - f;
+            const bool near = !(frac >= 0x1p-8 && frac <= 1.0 - 0x1p-8);
+            // One pass from the bottom.  X = Z0 + 2^8 Z1 + 2^16 Z2 + 2^24 Z3,
+            // Z_s the number whose limb l is D[4 l + s] (< 2^26), so limb l of
+            // 2^(8 s) Z_s is one funnel shift of Z_s[l - 1] and Z_s[l] and the
+            // limb's share of X is z0 + s1 + s2 + s3 < 2^34 with no products.
+            // e q enters as words: lo(e_lo q_l) + hi(e_lo q_(l-1)) +
+            // lo(e_hi q_(l-1)) + hi(e_hi q_(l-2)).  Both are formed off the
+            // carry chain; the chain itself is one signed 64-bit add a limb.
+            // TMEM pieces are double-buffered: piece pc + 1 loads while piece
+            // pc is used.
+            uint64_t pp = 0, hp = 0, hp2 = 0;
+            uint32_t z1p = 0, z2p = 0, z3p = 0;
+            int64_t cy = 0;
+            uint32_t o[4], over = 0;
             tc::tmem_ld16(tq, ra);
             tmem_wait(ra);
 #pragma unroll
@@ -491,36 +504,36 @@ __global__ void __launch_bounds__(kThreads, 1)
                 for (int ii = 0; ii < 4; ++ii) {
                     const int kl = 4 * pc + ii;
                     if (kl < kXL && kl < n) {
-                        // The limb's own terms (the D bytes, the top-limb words,
-                        // e q_k) do not depend on the carries: formed first, so
-                        // only 64-bit additions remain on the serial chain.
-                        uint64_t sd = 0;
-                        if (have) {
-                            sd = static_cast<uint64_t>(cur[4 * ii]) + (static_cast<uint64_t>(cur[4 * ii + 1]) << 8) +
-                                 (static_cast<uint64_t>(cur[4 * ii + 2]) << 16) +
-                                 (static_cast<uint64_t>(cur[4 * ii + 3]) << 24);
-                        }
+                        const uint32_t z0 = have ? cur[4 * ii] : 0u, z1 = have ? cur[4 * ii + 1] : 0u;
+                        const uint32_t z2 = have ? cur[4 * ii + 2] : 0u, z3 = have ? cur[4 * ii + 3] : 0u;
+                        uint64_t sd = static_cast<uint64_t>(z0) + __funnelshift_l(z1p, z1, 8) +
+                                      static_cast<uint64_t>(__funnelshift_l(z2p, z2, 16)) + __funnelshift_l(z3p, z3, 24);
+                        z1p = z1;
+                        z2p = z2;
+                        z3p = z3;
                         if (kl == L - 1) sd += meta.x;
                         if (kl == L) sd += meta.y;
                         if (kl == L + 1) sd += meta.z;
                         const uint32_t qk = sm.qs[kl];
-                        const uint64_t plo = static_cast<uint64_t>(e_lo) * qk, phi = static_cast<uint64_t>(e_hi) * qk;
-                        const uint64_t w = carry + sd;
-                        carry = w >> 32;
-                        const uint64_t acc = plo + c0;
-                        c0 = (acc >> 32) + phi;
-                        const uint64_t dy =
-                            static_cast<uint64_t>(static_cast<uint32_t>(w)) - static_cast<uint32_t>(acc) - b0;
-                        const uint32_t yk = static_cast<uint32_t>(dy);
-                        b0 = static_cast<uint32_t>(dy >> 63);
-                        b1 = static_cast<uint32_t>((static_cast<uint64_t>(yk) - qk - b1) >> 63);
+                        const uint64_t P = static_cast<uint64_t>(e_lo) * qk, H = static_cast<uint64_t>(e_hi) * qk;
+                        const uint64_t t = (P & 0xFFFFFFFFu) + (pp >> 32) + (hp & 0xFFFFFFFFu) + (hp2 >> 32);
+                        pp = P;
+                        hp2 = hp;
+                        hp = H;
+                        const int64_t v = static_cast<int64_t>(sd) - static_cast<int64_t>(t) + cy;
+                        cy = v >> 32;
+                        const uint32_t yk = static_cast<uint32_t>(v);
                         o[ii] = yk;
-                        if (kl < L && live) {
-                            if (gvec) {
-                                if (ii == 3) *reinterpret_cast<uint4*>(crow + kl - 3) = make_uint4(o[0], o[1], o[2], o[3]);
-                            } else {
-                                crow[kl] = yk;
+                        if (kl < L) {
+                            if (live) {
+                                if (gvec) {
+                                    if (ii == 3) *reinterpret_cast<uint4*>(crow + kl - 3) = make_uint4(o[0], o[1], o[2], o[3]);
+                                } else {
+                                    crow[kl] = yk;
+                                }
                             }
+                        } else {
+                            over |= yk;   // limbs L and L + 1 of a non-negative result
                         }
                     }
                 }
@@ -529,19 +542,33 @@ __global__ void __launch_bounds__(kThreads, 1)
             // TMEM is read: the MMAs of this buffer's next tile may start.
             tc::tc_fence_before();
             tc::mbar_arrive(&sm.d_empty[grp]);
-            // X - e q is negative (add q) or at least q (subtract q): rare.
-            if (live && (b0 || !b1)) {
-                uint32_t cb = 0;
-                for (int kk = 0; kk < L; ++kk) {
-                    const uint32_t x = crow[kk], qk = sm.qs[kk];
-                    if (b0) {
-                        const uint64_t sum = static_cast<uint64_t>(x) + qk + cb;
-                        crow[kk] = static_cast<uint32_t>(sum);
-                        cb = static_cast<uint32_t>(sum >> 32);
-                    } else {
-                        const uint64_t dd = static_cast<uint64_t>(x) - qk - cb;
-                        crow[kk] = static_cast<uint32_t>(dd);
-                        cb = static_cast<uint32_t>(dd >> 63);
+            // r = X - e q in [-q, 2q): negative (cy < 0) adds q; a row near an
+            // integer quotient subtracts q when r >= q (r past limb L - 1, or
+            // its low L limbs at least q).  Rare: a second pass over the row.
+            if (live && (cy < 0 || near)) {
+                bool sub = false;
+                if (cy >= 0) {
+                    sub = over != 0;
+                    if (!sub) {
+                        uint32_t cb = 0;
+                        for (int kk = 0; kk < L; ++kk)
+                            cb = static_cast<uint32_t>((static_cast<uint64_t>(crow[kk]) - sm.qs[kk] - cb) >> 63);
+                        sub = cb == 0;
+                    }
+                }
+                if (cy < 0 || sub) {
+                    uint32_t cb = 0;
+                    for (int kk = 0; kk < L; ++kk) {
+                        const uint32_t x = crow[kk], qk = sm.qs[kk];
+                        if (cy < 0) {
+                            const uint64_t sum = static_cast<uint64_t>(x) + qk + cb;
+                            crow[kk] = static_cast<uint32_t>(sum);
+                            cb = static_cast<uint32_t>(sum >> 32);
+                        } else {
+                            const uint64_t dd = static_cast<uint64_t>(x) - qk - cb;
+                            crow[kk] = static_cast<uint32_t>(dd);
+                            cb = static_cast<uint32_t>(dd >> 63);
+                        }
                     }
                 }
             }
