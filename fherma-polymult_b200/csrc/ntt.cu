@@ -487,16 +487,7 @@ constexpr size_t row_bar_offset() {
 // count so far, mod 2); the barrier is initialised by the kernel.
 // smem: this team's region (row_smem_t<LOGS>() bytes, 1024-byte aligned);
 // tbar: its tables barrier (initialised, count 1).
-// TMAIO (row lengths 2^9 .. 2^11, whole blocks): the block's rows also arrive
-// by bulk copies (natural order in the exchange tiles, read conflict-free by
-// round 0, whose lanes are the row's low five bits) and the results leave by
-// bulk copies from shared memory.
-template <int LOGS>
-constexpr bool row_tma_io_ok() {
-    return LOGS >= 9 && RP<LOGS, 0, SwzRow, row_pass_rb(LOGS)>::lo(0) >= 5;
-}
-
-template <int LOGS, bool LAZY, class TEAM = BlockTeam, bool TMAIO = false>
+template <int LOGS, bool LAZY, class TEAM = BlockTeam>
 __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, int j, uint32_t bx,
                                          uint32_t phase, uint32_t* smem, uint64_t* tbar) {
     using RG = RowGeom<LOGS>;
@@ -517,49 +508,24 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
     const RowTable<LOGS, RG::kStride, true, RG::kFlip> iw{tf};
     uint32_t* const tiles[2] = {ta, tb};
 
-    constexpr uint32_t kRowsHere = RG::G >= 2 ? RG::G : 1;   // rows of elements in the tile
-    static_assert(!TMAIO || row_tma_io_ok<LOGS>(), "bulk-copied rows need round-0 lanes on the row's low bits");
-    // The tables (and with TMAIO the rows) stream into shared memory while
-    // round 0 loads its elements.
-    if (TEAM::tid() < 32) {
-        if constexpr (TMAIO) {
-            const int lane = threadIdx.x & 31;
-            if (lane == 0) tc::mbar_arrive_expect_tx(tbar, 2 * kRowsHere * RG::S * 4);
-            __syncwarp();
-            for (uint32_t s = lane; s < 2 * kRowsHere; s += 32) {
-                const uint32_t slot = s % kRowsHere, o = s / kRowsHere;
-                const size_t row = static_cast<size_t>(row_of_slot<LOGS>(slot, u0, R)) * RG::S;
-                tc::bulk_g2s(tiles[o] + slot * RG::S, (o ? b : a) + row, RG::S * 4, tbar);
-            }
-        }
-        row_tables_bulk<LOGS>(tf, d, j, u0, tbar);
-    }
+    // The tables stream into shared memory while round 0 loads its elements.
+    if (TEAM::tid() < 32) row_tables_bulk<LOGS>(tf, d, j, u0, tbar);
     // Round 0 straight from global memory (the thread's E elements lie in one
-    // row), or from the rows' copies in natural order.
+    // row).
     {
         const uint32_t base = round_base<LOGS, 0, SwzRow, RB, 0>(TEAM::tid());
         constexpr int sh = RPR::lo(0);
         uint32_t v[2][E];
-        if constexpr (TMAIO) {
-            if (!tc::wait_parity(tbar, phase, d.wait_ns) && (TEAM::tid() & 31) == 0) atomicOr(d.err, 4u);
+        const size_t at = row_offset<LOGS>(base, u0, R);
 #pragma unroll
-            for (int k = 0; k < E; ++k) {
-                v[0][k] = ta[base + (k << sh)];
-                v[1][k] = tb[base + (k << sh)];
-            }
-        } else {
-            const size_t at = row_offset<LOGS>(base, u0, R);
-#pragma unroll
-            for (int k = 0; k < E; ++k) {
-                v[0][k] = a[at + (k << sh)];
-                v[1][k] = b[at + (k << sh)];
-            }
-            // The bound only guards against a copy that never lands: past it the
-            // error word gets bit 2 and the block goes on (with wrong twiddles).
-            if (!tc::wait_parity(tbar, phase, d.wait_ns) && (TEAM::tid() & 31) == 0) atomicOr(d.err, 4u);
+        for (int k = 0; k < E; ++k) {
+            v[0][k] = a[at + (k << sh)];
+            v[1][k] = b[at + (k << sh)];
         }
+        // The bound only guards against a copy that never lands: past it the
+        // error word gets bit 2 and the block goes on (with wrong twiddles).
+        if (!tc::wait_parity(tbar, phase, d.wait_ns) && (TEAM::tid() & 31) == 0) atomicOr(d.err, 4u);
         fwd_round<LOGS, 0, SwzRow, RB, 0, LAZY, 2>(v, base, fw, p);
-        if constexpr (TMAIO) TEAM::sync();   // every thread has read the natural order
 #pragma unroll
         for (int o = 0; o < 2; ++o) store_round<LOGS, 0, SwzRow, RB, 0>(tiles[o], v[o], base);
         TEAM::sync();
@@ -618,26 +584,9 @@ __device__ __forceinline__ void row_body(const DevPoint& d, uint32_t* A, uint32_
 #pragma unroll
             for (int k = 0; k < E; ++k) v[k] = reduce_once(v[k], p);
         }
-        if constexpr (TMAIO) {
-            // Natural order back into the tile, then one bulk copy per row.
-            TEAM::sync();
+        const size_t at = row_offset<LOGS>(base, u0, R);
 #pragma unroll
-            for (int k = 0; k < E; ++k) ta[base + (k << sh)] = v[k];
-            tc::fence_proxy_async_smem();
-            TEAM::sync();
-            if (TEAM::tid() == 0) {
-                for (uint32_t slot = 0; slot < kRowsHere; ++slot) {
-                    const size_t row = static_cast<size_t>(row_of_slot<LOGS>(slot, u0, R)) * RG::S;
-                    tc::bulk_s2g(a + row, ta + slot * RG::S, RG::S * 4);
-                }
-                tc::bulk_commit();
-                tc::bulk_wait_read();   // the tile may be reused or the block may end
-            }
-        } else {
-            const size_t at = row_offset<LOGS>(base, u0, R);
-#pragma unroll
-            for (int k = 0; k < E; ++k) a[at + (k << sh)] = v[k];
-        }
+        for (int k = 0; k < E; ++k) a[at + (k << sh)] = v[k];
     }
 }
 
@@ -693,7 +642,7 @@ __global__ void __launch_bounds__(col_threads<LOGR>(), (col_min_blocks<LOGR, 6>(
     col_inv_body<LOGR, LOGS, LAZY>(d, A, blockIdx.y, blockIdx.x);
 }
 
-template <int LOGS, bool LAZY, bool TMAIO = false>
+template <int LOGS, bool LAZY>
 __global__ void __launch_bounds__(row_threads<LOGS>(), (row_min_blocks<LOGS>())) k_ntt_row(DevPoint d, uint32_t* A, uint32_t* B, int mode) {
     extern __shared__ __align__(1024) uint32_t smem[];
     uint64_t* tbar = reinterpret_cast<uint64_t*>(reinterpret_cast<uint8_t*>(smem) + row_bar_offset<LOGS>());
@@ -704,7 +653,7 @@ __global__ void __launch_bounds__(row_threads<LOGS>(), (row_min_blocks<LOGS>()))
     __syncthreads();
     pdl_launch_dependents();
     pdl_wait();
-    row_body<LOGS, LAZY, BlockTeam, TMAIO>(d, A, B, mode, blockIdx.y, blockIdx.x, 0, smem, tbar);
+    row_body<LOGS, LAZY, BlockTeam>(d, A, B, mode, blockIdx.y, blockIdx.x, 0, smem, tbar);
 }
 
 // Grouped launches over products of one geometry class: a (possibly
@@ -919,10 +868,6 @@ void row_attrs() {
     const int bytes = static_cast<int>(row_smem_t<LOGS>());
     check(cudaFuncSetAttribute(k_ntt_row<LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
           "row smem");
-    if constexpr (row_tma_io_ok<LOGS>()) {
-        check(cudaFuncSetAttribute(k_ntt_row<LOGS, LAZY, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
-              "row smem");
-    }
     check(cudaFuncSetAttribute(k_ntt_row_group<LOGS, LAZY>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes),
           "row smem");
 }
@@ -1045,16 +990,18 @@ CUtensorMap col_tmap(const DevPoint& d, const uint32_t* X) {
     return make_tmap_u32(X, static_cast<uint64_t>(d.K) << 6, d.N >> 6, d.N >> 6, 64, 32, TmaSwizzle::k128B);
 }
 
-// Column-pass variant: FPM_COL_PASS = tma1 (TMA, one tile per CTA; the
-// default), tma2 (TMA, persistent, two buffers) or plain (per-thread loads
-// and stores), read once.
+// Column-pass variant: FPM_COL_PASS = plain (per-thread loads and stores;
+// the default, measured fastest: at N = 65536, K = 139 the forward and
+// inverse passes take 21.8 and 13.2 us against 23.5 and 14.0 for tma1 and
+// 25.4 and 14.3 for tma2), tma1 (TMA, one tile per CTA) or tma2 (TMA,
+// persistent, two buffers), read once.
 int col_pass_variant() {
     static const int v = [] {
         const char* e = std::getenv("FPM_COL_PASS");
-        if (!e) return 1;
-        if (!std::strcmp(e, "plain")) return 0;
+        if (!e) return 0;
+        if (!std::strcmp(e, "tma1")) return 1;
         if (!std::strcmp(e, "tma2")) return 2;
-        return 1;
+        return 0;
     }();
     return v;
 }
@@ -1116,30 +1063,11 @@ void launch_col_inv_t(const DevPoint& d, uint32_t* A, cudaStream_t st) {
     });
 }
 
-// Row-pass variant: FPM_ROW_PASS = tma (rows in and out by bulk copies where
-// the row length allows) or plain (per-thread loads and stores; the
-// default), read once.
-bool row_pass_tma() {
-    static const bool v = [] {
-        const char* e = std::getenv("FPM_ROW_PASS");
-        return e && !std::strcmp(e, "tma");
-    }();
-    return v;
-}
-
 template <int LOGS, bool LAZY>
 void launch_row_t(const DevPoint& d, uint32_t* A, uint32_t* B, int mode, cudaStream_t st) {
     using RG = RowGeom<LOGS>;
     const uint32_t R = 1u << d.logR;
     const dim3 grid(RG::G >= 2 ? R / RG::G : R, d.K);
-    if constexpr (row_tma_io_ok<LOGS>()) {
-        if (row_pass_tma() && (reinterpret_cast<uintptr_t>(A) & 15) == 0 && (reinterpret_cast<uintptr_t>(B) & 15) == 0) {
-            check(launch_pdl(k_ntt_row<LOGS, LAZY, true>, grid, dim3(row_threads<LOGS>()), row_smem_t<LOGS>(), st, d,
-                             A, B, mode),
-                  "row launch");
-            return;
-        }
-    }
     check(launch_pdl(k_ntt_row<LOGS, LAZY>, grid, dim3(row_threads<LOGS>()), row_smem_t<LOGS>(), st, d, A, B, mode),
           "row launch");
 }
