@@ -218,8 +218,9 @@ int fpm_get_crt_tables(const fpm_ctx* ctx, uint32_t* M, uint32_t* negvP) {
 }
 
 int fpm_stage_decompose(fpm_ctx* ctx, const uint32_t* d_limbs, uint32_t* d_res, int operand, void* stream) {
-    if (!ctx || !d_limbs || !d_res || (operand != 0 && operand != 1))
+    if (!ctx || !d_limbs || !d_res || operand < 0 || operand > 2)
         return fail(FPM_EINVAL, "fpm_stage_decompose: bad argument");
+    if (operand == 2) return guarded([&] { ctx->engine->decompose_pair(d_limbs, d_res, as_stream(stream)); });
     return guarded([&] { ctx->engine->decompose(d_limbs, d_res, operand, as_stream(stream)); });
 }
 

@@ -299,6 +299,26 @@ void Engine::transform(uint32_t* d_A, uint32_t* d_B, int mode, cudaStream_t st) 
     check(cudaGetLastError(), "transform launch");
 }
 
+// Both operands' decompose, as a product launches it (one paired launch on the
+// tensor-core paths).
+void Engine::decompose_pair_on(const DevPoint& d, const uint32_t* a, const uint32_t* b, uint32_t* A, uint32_t* B,
+                               cudaStream_t st) {
+    if (simt_) {
+        launch_decompose(d, a, A, 0, 0, plan_.N, st);
+        launch_decompose(d, b, B, 1, 0, plan_.N, st);
+    } else if (dec_consts_) {
+        launch_decompose_pipe(d, *dec_consts_, a, b, A, B, 0, 0, plan_.N, sms_, st);
+    } else {
+        launch_decompose_tc_pair(d, a, b, A, B, st);
+    }
+}
+
+void Engine::decompose_pair(const uint32_t* d_limbs, uint32_t* d_res, cudaStream_t st) {
+    const size_t nl = static_cast<size_t>(plan_.N) * plan_.L, kn = static_cast<size_t>(plan_.K) * plan_.N;
+    decompose_pair_on(dp_, d_limbs, d_limbs + nl, d_res, d_res + kn, st);
+    check(cudaGetLastError(), "decompose launch");
+}
+
 void Engine::crt(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st) {
     launch_crt_any(dp_, d_y, d_c, 0, plan_.N, st);
     check(cudaGetLastError(), "crt launch");
@@ -307,14 +327,7 @@ void Engine::crt(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st) {
 void Engine::product(const DevPoint& d, const uint32_t* d_a, const uint32_t* d_b, uint32_t* A, uint32_t* B,
                      uint32_t* d_c, cudaStream_t st) {
     const uint32_t N = plan_.N;
-    if (simt_) {
-        launch_decompose(d, d_a, A, 0, 0, N, st);
-        launch_decompose(d, d_b, B, 1, 0, N, st);
-    } else if (dec_consts_) {
-        launch_decompose_pipe(d, *dec_consts_, d_a, d_b, A, B, 0, 0, N, sms_, st);
-    } else {
-        launch_decompose_tc_pair(d, d_a, d_b, A, B, st);
-    }
+    decompose_pair_on(d, d_a, d_b, A, B, st);
     launch_ntt(d, A, B, kRowProduct, st);
     launch_crt_any(d, A, d_c, 0, N, st);
     check(cudaGetLastError(), "product launch");

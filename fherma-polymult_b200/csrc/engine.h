@@ -64,6 +64,8 @@ public:
 
     // Stages, for checks against the oracle.
     void decompose(const uint32_t* d_limbs, uint32_t* d_res, int operand, cudaStream_t st);
+    // Both operands in one launch: d_limbs = a then b, d_res = A then B.
+    void decompose_pair(const uint32_t* d_limbs, uint32_t* d_res, cudaStream_t st);
     void transform(uint32_t* d_A, uint32_t* d_B, int mode, cudaStream_t st);
     void crt(const uint32_t* d_y, uint32_t* d_c, cudaStream_t st);
 
@@ -101,6 +103,8 @@ private:
     void product(const DevPoint& d, const uint32_t* d_a, const uint32_t* d_b, uint32_t* A, uint32_t* B, uint32_t* d_c,
                  cudaStream_t st);
     void release();
+    void decompose_pair_on(const DevPoint& d, const uint32_t* a, const uint32_t* b, uint32_t* A, uint32_t* B,
+                           cudaStream_t st);
     void launch_dec(const uint32_t* d_limbs, uint32_t* d_res, int operand, uint32_t n0, uint32_t n1,
                     cudaStream_t st);
     void launch_crt_any(const DevPoint& d, const uint32_t* d_y, uint32_t* d_c, uint32_t n0, uint32_t n1,

@@ -164,7 +164,9 @@ FPM_API int fpm_get_crt_tables(const fpm_ctx* ctx, uint32_t* M, uint32_t* negvP)
  *              N^-1 (P/p_j)^-1 2^32 (reference k_decompose, solve.cu:98-126).
  *              With 30-bit primes and N > 1024 the values are left below
  *              4 p_j (congruent; the transform's first butterflies are lazy),
- *              otherwise they are canonical;
+ *              otherwise they are canonical; operand 2 does both in the one
+ *              launch a product uses: d_limbs holds a then b (2 N L words),
+ *              d_res receives A then B (2 K N words);
  *   transform: mode 0: A, B -> y_j = INTT(NTT(A) NTT(B)) in A (reference
  *              k_ntt_cols / k_ntt_rows_mul, solve.cu:130-233); mode 1: forward
  *              transforms of A and B in place, bit-reversed order;

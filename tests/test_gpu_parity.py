@@ -93,6 +93,12 @@ def test_stages_match_oracle(cuda, N, W, prime_bits):
         for got, want, what in ((host(A), ra, "decompose a"), (host(B), scaled(pl, rb, N), "decompose b (scaled)")):
             assert (got.astype(np.uint64) < bound * pj).all(), what + ": range"
             assert np.array_equal(got.astype(np.uint64) % pj, want.astype(np.uint64)), what
+        # The paired launch a product uses (operand 2: a then b in, A then B out).
+        AB = torch.zeros((2 * K, N), dtype=torch.int32, device="cuda")
+        lab = torch.cat((da, db))
+        ctx.stage_decompose(lab.data_ptr(), AB.data_ptr(), 2)
+        torch.cuda.synchronize()
+        assert np.array_equal(host(AB[:K]), host(A)) and np.array_equal(host(AB[K:]), host(B)), "paired decompose"
         rb_s = scaled(pl, rb, N)
 
         ctx.stage_transform(A.data_ptr(), B.data_ptr(), polymul.MODE_FORWARD)
