@@ -109,7 +109,10 @@ static_assert(kMaxL <= 64, "D_0 + 2^8 D_1 must fit 32 bits");
 template <bool LAZY>
 __device__ __forceinline__ uint32_t fold_halves(uint32_t A, uint32_t B, uint4 f) {
     if constexpr (LAZY) {
-        return shoup_lazy(A, 1u, f.w, f.x) + shoup_lazy(B, f.y, f.z, f.x);
+        // (A - q1 p) + (B f.y - q2 p), each term in [0, 2p) (Shoup): one
+        // product by p for both quotients, the same value below 4p.
+        const uint32_t q = mulhi32(A, f.w) + mulhi32(B, f.z);
+        return B * f.y + A - q * f.x;
     } else {
         return add_mod(shoup(A, 1u, f.w, f.x), shoup(B, f.y, f.z, f.x), f.x);
     }
