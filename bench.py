@@ -20,7 +20,9 @@ roofline: the dominant kernel's algorithmic bytes per launch over its CUDA-event
 cpu_baseline: the reference's own CPU implementation (solve_cpu.cpp, OpenMP,
          built into oracle/_ref/) on a bounded sample, rank 0 only.
 batched: 64 products of the uneven mix (N 4096 .. 65536, W 128 .. 2048) as one
-         autotuned graph of grouped launches, against 64 sequential plain calls;
+         autotuned graph of grouped launches, against 64 sequential plain calls
+         (device against device, host against host); stage_launch_layout is
+         the five-launch schedule (one grouped launch per stage) timed alike;
          batched_n65536: the same for 16 products at N = 65536 (W 1747 / 2048).
 serving: a seeded Poisson stream (10,000 requests at 2000/s) through the
          serving loop; p50 / p99 latency and products/s.
@@ -393,6 +395,19 @@ def measure_batched(torch, polymul, workload, stream, count=64, reps=20, mix="un
     seq_e2e_us = (time.perf_counter() - t0) * 1e6
     exact = all(np.array_equal(g, o) for g, o in zip(got, outs)) and all(
         np.array_equal(x, o) for x, o in zip(pc, outs))
+    # The one-launch-per-stage layout (3, every product in grouped launches:
+    # decompose, the three transform passes over all products, CRT), timed
+    # the same way, with its best grid, whether or not the tuner chose it.
+    stage_layout = None
+    for grid in (0, 1):
+        bt.set_schedule(layout=3, order=1, prime_group=0, grid=grid, pipe_min_log_n=0)
+        us3 = timed(lambda: bt.run_device(sp), reps)
+        if stage_layout is None or us3 < stage_layout["batch_us"]:
+            stage_layout = {"layout": 3, "grid": grid, "batch_us": us3, "launches_per_batch": bt.info.launches,
+                            "speedup_vs_sequential": seq_us / us3}
+    bt.set_schedule(layout=3, order=1, prime_group=0, grid=stage_layout["grid"], pipe_min_log_n=0)
+    c3 = [x.copy() for x in bt.run(pa, pb)]
+    stage_layout["bit_exact_vs_plain"] = bool(all(np.array_equal(x, o) for x, o in zip(c3, outs)))
     res = {
         "products": count,
         "mix": ("N = 65536, W alternating 1747 / 2048, seed 3300" if mix == "n65536" else
@@ -406,6 +421,7 @@ def measure_batched(torch, polymul, workload, stream, count=64, reps=20, mix="un
         "schedule": {"layout": info.layout, "order": info.order, "prime_group": info.prime_group,
                      "grid": info.grid, "pipe_min_log_n": info.pipe_min_log_n, "tuned_us": info.tuned_us},
         "launches_per_batch": info.launches, "device_bytes": info.device_bytes, "bit_exact_vs_plain": bool(exact),
+        "stage_launch_layout": stage_layout,
     }
     bt.close()
     for c in ctxs:
