@@ -14,8 +14,9 @@
 //     256-column TMEM buffers;
 //   * warps 1-4 copy each tile's limbs into a two-slot ring in the MMA's
 //     128-byte-swizzled K-major layout (the layout the tensor cores read at
-//     full rate) with asynchronous copies (cp.async), one tile in flight
-//     while the previous one lands and is multiplied: a warp moves 8 rows x 4
+//     full rate) with asynchronous copies (cp.async) whose completion the
+//     slot's mbarrier tracks (cp.async.mbarrier.arrive), so a slot is handed
+//     to the MMAs the moment its copies land: a warp moves 8 rows x 4
 //     sixteen-byte groups at a time, so the global loads are 64-byte runs and
 //     the eight lanes of each shared-store phase hit eight different bank
 //     groups;
@@ -94,6 +95,11 @@ __device__ __forceinline__ void cp_async4_zfill(void* dst, const void* src, bool
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// One arrival on `bar` once every cp.async this thread issued so far has
+// completed (the barrier's count includes it: .noinc).
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(tc::smem_addr(bar)) : "memory");
+}
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
@@ -192,6 +198,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                 const int s = i & 1;
                 ok = tc::wait_or_abort(&sm.a_full[s], (i >> 1) & 1, sm.abort, lim);
                 if (!ok) break;
+                // The limbs came through the generic proxy (cp.async).
+                tc::fence_proxy_async_smem();
                 const uint32_t a0 = tc::smem_addr(sm.a + s * a_bytes(kb));
                 for (int c = 0; c < nch; ++c, ++g) {
                     const int buf = g & 1;
@@ -270,20 +278,14 @@ __global__ void __launch_bounds__(kThreads, 1)
                     cp_async4_zfill(at + sw128_offset(mm, 4 * l, kRows), have ? src + mm * L + l : src, have);
                 }
             }
+            // The slot's barrier completes when this thread's copies have
+            // landed (the hardware arrives for it), so the loader goes on to
+            // the next slot at once; the MMA issuer fences the async proxy.
             cp_async_commit();
-            if (i >= 1) {
-                // The previous tile's copies have landed: hand it to the MMAs.
-                cp_async_wait<1>();
-                tc::fence_proxy_async_smem();
-                tc::mbar_arrive(&sm.a_full[s ^ 1]);
-            }
+            cp_async_arrive_noinc(&sm.a_full[s]);
         }
-        // The last tile (and, after an abort, whatever is still in flight).
+        // Whatever is still in flight lands before the CTA may exit.
         cp_async_wait<0>();
-        if (ok && i >= 1) {
-            tc::fence_proxy_async_smem();
-            tc::mbar_arrive(&sm.a_full[(i - 1) & 1]);
-        }
     } else {
         // ---- epilogue: thread = one coefficient, 16 primes of each chunk ----
         const int ew = warp - kEpiWarp0;
