@@ -311,12 +311,17 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tc::tc_fence_before();
                 tc::mbar_arrive(&sm.d_empty[buf]);
                 if (j0 < K) {
+                    // One running pointer down the primes' rows (no 64-bit
+                    // product per store).
+                    uint32_t* out = res + static_cast<size_t>(j0) * d.N + n0 + m;
+                    const size_t stride = d.N;
 #pragma unroll
                     for (int k = 0; k < 16; ++k) {
                         const int j = j0 + k;
                         const uint32_t* rr = r[k >> 3] + 4 * (k & 7);
                         const uint32_t A = rr[0] + (rr[1] << 8), B = rr[2] + (rr[3] << 8);
-                        if (live && j < K) res[static_cast<size_t>(j) * d.N + n0 + m] = fold_halves<LAZY>(A, B, fc.fold[j]);
+                        if (live && j < K) *out = fold_halves<LAZY>(A, B, fc.fold[j]);
+                        out += stride;
                     }
                 }
             }
