@@ -14,7 +14,7 @@ value  : device-only, operands resident in HBM; four operand sets rotate so the
          inputs of consecutive steps (4 x 50 MB) are larger than L2 (126 MB).
 e2e    : the same product through the public C API with host buffers
          (fpm_run: host->device copies of a and b, device->host copy of c,
-         inside the timed region), wall clock.
+         inside the timed region), wall clock per call, median of 50 calls.
 roofline: the dominant kernel's algorithmic bytes per launch over its CUDA-event
          duration, against the measured HBM copy bandwidth.
 cpu_baseline: the reference's own CPU implementation (solve_cpu.cpp, OpenMP,
@@ -630,16 +630,20 @@ def main():
     c_pt, c_p = pinned(np.zeros((N, L), np.uint32))
 
     def e2e(a_, b_, c_, n):
+        """Median and mean of n calls, each timed by wall clock around fpm_run
+        (a host-side stall in one call moves the mean, not the median)."""
         ctx.run(a_, b_, c_)
-        t0 = time.perf_counter()
+        ts = []
         for _ in range(n):
+            t0 = time.perf_counter()
             ctx.run(a_, b_, c_)
-        return (time.perf_counter() - t0) * 1e6 / n
+            ts.append((time.perf_counter() - t0) * 1e6)
+        return statistics.median(ts), statistics.fmean(ts)
 
     io_chunks = ctx.tune_host_path()   # as fherma_init does, outside the timed calls
-    e2e_us = e2e(a_p, b_p, c_p, args.e2e_steps)
+    e2e_us, e2e_mean_us = e2e(a_p, b_p, c_p, args.e2e_steps)
     c_h = np.empty((N, L), np.uint32)
-    e2e_pageable_us = e2e(a_h, b_h, c_h, args.e2e_steps)
+    e2e_pageable_us, _ = e2e(a_h, b_h, c_h, args.e2e_steps)
 
     # The link itself: pinned copies of one product's operands in and result
     # out, timed alone with CUDA events (best of 5).  Their sum plus the device
@@ -765,6 +769,7 @@ def main():
             "products_per_s": 1e6 / us_per_product,
             "e2e": {"value": e2e_us, "unit": "us/product", "h2d_bytes_per_step": 2 * N * L * 4,
                     "d2h_bytes_per_step": N * L * 4, "host_buffers": "pinned (fpm_run, wall clock)",
+                    "statistic": "median of the calls (mean_us beside it)", "mean_us": e2e_mean_us,
                     "io_chunks": io_chunks, "calls": args.e2e_steps},
             "e2e_pageable": {"value": e2e_pageable_us, "unit": "us/product",
                              "host_buffers": "pageable numpy (fpm_run stages through pinned memory)"},
