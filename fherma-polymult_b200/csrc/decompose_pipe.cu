@@ -105,6 +105,19 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// Waits for this thread's two 32-column TMEM loads; naming the registers
+// keeps every read of them below the wait.
+#define FPM_R16(x, o) "+r"(x[o + 0]), "+r"(x[o + 1]), "+r"(x[o + 2]), "+r"(x[o + 3]), "+r"(x[o + 4]), \
+    "+r"(x[o + 5]), "+r"(x[o + 6]), "+r"(x[o + 7]), "+r"(x[o + 8]), "+r"(x[o + 9]), "+r"(x[o + 10]), \
+    "+r"(x[o + 11]), "+r"(x[o + 12]), "+r"(x[o + 13]), "+r"(x[o + 14]), "+r"(x[o + 15])
+__device__ __forceinline__ void tmem_wait2(uint32_t (&r)[2][32]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;" : FPM_R16(r[0], 0)::"memory");
+    asm volatile("" : FPM_R16(r[0], 16)::"memory");
+    asm volatile("" : FPM_R16(r[1], 0)::"memory");
+    asm volatile("" : FPM_R16(r[1], 16)::"memory");
+}
+#undef FPM_R16
+
 // A GEMM sum D is below 4L 255^2 <= 256 * 65025 (L <= 64), so both halves of
 // sum_s D_s 2^(8s), A = D_0 + 2^8 D_1 and B = D_2 + 2^8 D_3, are below
 // 257 * 256 * 65025 < 2^32, and the residue is (A + B 2^16) mod p:
@@ -307,7 +320,16 @@ __global__ void __launch_bounds__(kThreads, 1)
                 uint32_t r[2][32];
                 tc::tmem_ld32(tq + buf * kCols, r[0]);
                 tc::tmem_ld32(tq + buf * kCols + 32, r[1]);
-                tc::tmem_ld_wait();
+                tmem_wait2(r);
+                // The 32 half-sums are formed before the buffer is released:
+                // half as many values stay live through the folds.
+                uint32_t hs[16][2];
+#pragma unroll
+                for (int k = 0; k < 16; ++k) {
+                    const uint32_t* rr = r[k >> 3] + 4 * (k & 7);
+                    hs[k][0] = rr[0] + (rr[1] << 8);
+                    hs[k][1] = rr[2] + (rr[3] << 8);
+                }
                 tc::tc_fence_before();
                 tc::mbar_arrive(&sm.d_empty[buf]);
                 if (j0 < K) {
@@ -318,9 +340,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                     for (int k = 0; k < 16; ++k) {
                         const int j = j0 + k;
-                        const uint32_t* rr = r[k >> 3] + 4 * (k & 7);
-                        const uint32_t A = rr[0] + (rr[1] << 8), B = rr[2] + (rr[3] << 8);
-                        if (live && j < K) *out = fold_halves<LAZY>(A, B, fc.fold[j]);
+                        if (live && j < K) *out = fold_halves<LAZY>(hs[k][0], hs[k][1], fc.fold[j]);
                         out += stride;
                     }
                 }
