@@ -241,7 +241,7 @@ def n65536_points(count, seed):
     return [(65536, (1747, 2048)[i % 2], None) for i in range(count)], rng
 
 
-# The benchmark points and their value distributions.
+# The other benchmark points (N, W) and their value distributions.
 CONFIG_POINTS = [
     ("N4096_W256", "uniform"),
     ("N32768_W868", "uniform"), ("N32768_W868", "max"), ("N32768_W868", "sparse"),
