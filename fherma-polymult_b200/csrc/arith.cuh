@@ -154,6 +154,7 @@ FPM_HD uint32_t bitrev(uint32_t x, uint32_t bits) {
 // above them.
 
 FPM_HD bool limbs_geq(const uint32_t* x, int n, const uint32_t* q, int L) {
+#pragma unroll
     for (int i = n - 1; i >= 0; --i) {
         const uint32_t qi = i < L ? q[i] : 0u;
         if (x[i] != qi) return x[i] > qi;
@@ -164,6 +165,7 @@ FPM_HD bool limbs_geq(const uint32_t* x, int n, const uint32_t* q, int L) {
 // x -= q (x >= q).
 FPM_HD void limbs_sub(uint32_t* x, int n, const uint32_t* q, int L) {
     uint32_t borrow = 0;
+#pragma unroll
     for (int i = 0; i < n; ++i) {
         const uint64_t d = static_cast<uint64_t>(x[i]) - (i < L ? q[i] : 0u) - borrow;
         x[i] = static_cast<uint32_t>(d);
@@ -175,6 +177,7 @@ FPM_HD void limbs_sub(uint32_t* x, int n, const uint32_t* q, int L) {
 FPM_HD void limbs_submul(uint32_t* x, int n, const uint32_t* q, int L, uint32_t e, int shift) {
     uint64_t carry = 0;
     uint32_t borrow = 0;
+#pragma unroll
     for (int i = shift; i < n; ++i) {
         const int k = i - shift;
         const uint64_t prod = (k < L ? static_cast<uint64_t>(e) * q[k] : 0u) + carry;
@@ -203,6 +206,7 @@ inline double modulus_top(const uint32_t* q, int L) {
 // (Same method as the reference's reduce_wide, rns.cuh:204-221.)
 FPM_HD void reduce_mod_q(uint32_t* x, int n, const uint32_t* q, int L, double q_top) {
     double xd = 0;
+#pragma unroll
     for (int i = n - 1; i >= top_drop(L); --i) xd = xd * 4294967296.0 + x[i];
     const double f = floor(xd / q_top);
     const uint64_t e = f >= 1 ? static_cast<uint64_t>(f) - 1 : 0;

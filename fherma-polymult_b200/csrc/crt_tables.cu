@@ -20,9 +20,15 @@ namespace fpm {
 
 namespace {
 
-// x (L limbs, x < q) = x * m mod q; t is scratch of L + 1 limbs.
-__device__ void mul_word_mod(uint32_t* x, uint32_t m, const uint32_t* q, int L, double q_top, uint32_t* t) {
+// x (L limbs, x < q) = x * m mod q; t is scratch of L + 1 limbs.  LT > 0:
+// L = LT at compile time, so every loop unrolls and x and t stay in
+// registers (with a run-time L they live in local memory).
+template <int LT>
+__device__ __forceinline__ void mul_word_mod(uint32_t* x, uint32_t m, const uint32_t* q, int Lrt, double q_top,
+                                             uint32_t* t) {
+    const int L = LT > 0 ? LT : Lrt;
     uint64_t carry = 0;
+#pragma unroll
     for (int l = 0; l < L; ++l) {
         const uint64_t v = static_cast<uint64_t>(x[l]) * m + carry;
         t[l] = static_cast<uint32_t>(v);
@@ -30,20 +36,26 @@ __device__ void mul_word_mod(uint32_t* x, uint32_t m, const uint32_t* q, int L, 
     }
     t[L] = static_cast<uint32_t>(carry);
     reduce_mod_q(t, L + 1, q, L, q_top);
+#pragma unroll
     for (int l = 0; l < L; ++l) x[l] = t[l];
 }
 
 // Thread j < K: M_j.  Thread K: P mod q (into Pq).
-__global__ void k_crt_products(const PrimeConsts* pc, int K, const uint32_t* q, int L, double q_top, uint32_t* M,
+template <int LT>
+__global__ void k_crt_products(const PrimeConsts* pc, int K, const uint32_t* q, int Lrt, double q_top, uint32_t* M,
                                uint32_t* Pq) {
+    const int L = LT > 0 ? LT : Lrt;
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j > K) return;
-    uint32_t x[kMaxL], t[kMaxL + 1];
+    constexpr int kL = LT > 0 ? LT : kMaxL;
+    uint32_t x[kL], t[kL + 1];
+#pragma unroll
     for (int l = 0; l < L; ++l) x[l] = l == 0 ? 1u : 0u;
     for (int i = 0; i < K; ++i) {
-        if (i != j) mul_word_mod(x, pc[i].p, q, L, q_top, t);
+        if (i != j) mul_word_mod<LT>(x, pc[i].p, q, L, q_top, t);
     }
     uint32_t* out = j < K ? M + static_cast<size_t>(j) * L : Pq;
+#pragma unroll
     for (int l = 0; l < L; ++l) out[l] = x[l];
 }
 
@@ -53,7 +65,7 @@ __global__ void k_crt_negvp(const uint32_t* Pq, int K, const uint32_t* q, int L,
     if (v > K) return;
     uint32_t x[kMaxL], t[kMaxL + 1];
     for (int l = 0; l < L; ++l) x[l] = Pq[l];
-    mul_word_mod(x, static_cast<uint32_t>(v), q, L, q_top, t);
+    mul_word_mod<0>(x, static_cast<uint32_t>(v), q, L, q_top, t);
     bool zero = true;
     for (int l = 0; l < L; ++l) zero = zero && x[l] == 0;
     uint32_t* out = negvP + static_cast<size_t>(v) * L;
@@ -92,7 +104,16 @@ size_t crt_image_bytes(const HostPlan& pl, int rows) {
 void build_crt_tables(const HostPlan& pl, const PrimeConsts* pc, const uint32_t* q, uint32_t* M, uint32_t* negvP,
                       uint32_t* Pq, uint8_t* img, uint8_t* img_v, cudaStream_t st) {
     const int K = pl.K, L = pl.L;
-    k_crt_products<<<(K + 1 + 63) / 64, 64, 0, st>>>(pc, K, q, L, pl.q_top, M, Pq);
+    // One thread per j runs K - 1 word products in sequence: small blocks
+    // spread the K + 1 threads over SMs.
+    const dim3 pg((K + 1 + 31) / 32), pb(32);
+    switch (L) {
+        case 64: k_crt_products<64><<<pg, pb, 0, st>>>(pc, K, q, L, pl.q_top, M, Pq); break;
+        case 55: k_crt_products<55><<<pg, pb, 0, st>>>(pc, K, q, L, pl.q_top, M, Pq); break;
+        case 28: k_crt_products<28><<<pg, pb, 0, st>>>(pc, K, q, L, pl.q_top, M, Pq); break;
+        case 8: k_crt_products<8><<<pg, pb, 0, st>>>(pc, K, q, L, pl.q_top, M, Pq); break;
+        default: k_crt_products<0><<<pg, pb, 0, st>>>(pc, K, q, L, pl.q_top, M, Pq); break;
+    }
     check(cudaGetLastError(), "crt tables launch");
     k_crt_negvp<<<(K + 1 + 63) / 64, 64, 0, st>>>(Pq, K, q, L, pl.q_top, negvP);
     check(cudaGetLastError(), "crt tables launch");
