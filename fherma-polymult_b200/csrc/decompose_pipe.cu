@@ -12,7 +12,7 @@
 //     resident in shared memory) and then, one thread, issues the MMAs at the
 //     widest shape (N = 256 columns per chunk): D goes to one of two
 //     256-column TMEM buffers;
-//   * warps 1-4 copy each tile's limbs into a two-slot ring in the MMA's
+//   * warps 1-4 copy each tile's limbs into a ring of two slots in the MMA's
 //     128-byte-swizzled K-major layout (the layout the tensor cores read at
 //     full rate) with asynchronous copies (cp.async) whose completion the
 //     slot's mbarrier tracks (cp.async.mbarrier.arrive), so a slot is handed

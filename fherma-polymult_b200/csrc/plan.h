@@ -86,7 +86,9 @@ struct HostPlan {
     uint32_t dec_chunks = 0;                 // ceil(K / 32)
     std::vector<uint8_t> dec_img_a, dec_img_b;
     // The same constants in chunks of 64 primes (256 columns) for the
-    // pipelined decompose; the last chunk has dec_wlast columns.
+    // pipelined decompose, in the UMMA K-major 128-byte-swizzle layout
+    // (sw128_offset, one block per 128 K bytes); the last chunk has
+    // dec_wlast columns.
     uint32_t dec_wchunks = 0, dec_wlast = 0;
     std::vector<uint8_t> dec_wimg_a, dec_wimg_b;
     std::vector<uint4> dec_fold;             // K: {p, 2^16 mod p, its Shoup companion, floor(2^32 / p)}
@@ -100,6 +102,8 @@ struct HostPlan {
     std::vector<uint8_t> crt_img;
     // The same image with a row K for -P mod q (= negvP_1), and that
     // constant's top limb: the pipelined CRT multiplies it by v in the GEMM.
+    // Laid out for that kernel (crt_image_at with swz): every 32-prime chunk
+    // but the last 128-byte swizzled, the last in core matrices.
     std::vector<uint8_t> crt_img_v;
     uint32_t negp_top = 0;
 };
