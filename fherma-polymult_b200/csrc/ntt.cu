@@ -607,10 +607,12 @@ constexpr int col_min_blocks() {
     return col_pass_rb(LOGR) == 3 ? MIN8 : 8;
 }
 // Row kernels: five blocks of 256 threads (8-element rounds, 48 registers), or
-// six of 128 (16-element rounds, 80 registers: 64 spills).
+// five of 128 (16-element rounds, up to 96 registers).  At N = 65536 (K = 139)
+// the 16-element row pass measured 54.9 us with five blocks per SM against
+// 56.4 with six (80 registers) and 54.5 with four; 64 registers spill.
 template <int LOGS>
 constexpr int row_min_blocks() {
-    return row_pass_rb(LOGS) == 3 ? 5 : 6;
+    return 5;
 }
 
 // Blocks per prime of each pass.
